@@ -1,0 +1,53 @@
+"""Build libbgt.so (sm_100a) in-tree: bmad-ecosystem_b200/bgt/libbgt.so.
+
+    python bmad-ecosystem_b200/build.py [--fmad]
+
+--fmad lets nvcc contract a*b+c into FMA (off by default: the reference's
+gfortran -O2 x86-64 build never contracts, and parity is checked against
+that operation order).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "csrc" / "bgt_track.cu"
+OUT = HERE / "bgt" / "libbgt.so"
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.sep not in c or Path(c).exists()):
+            return c
+    return "nvcc"
+
+
+def build(fmad: bool = False, out: Path = OUT, verbose: bool = False) -> Path:
+    deps = list((HERE / "csrc").glob("*")) + [HERE.parent / "include" / "bgt.h"]
+    if out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps) and not os.environ.get(
+            "BGT_FORCE_BUILD"):
+        return out
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+           f"--fmad={'true' if fmad else 'false'}", "-Xcompiler", "-fPIC", "-shared", "-o", str(out), str(SRC),
+           "-lquadmath"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building libbgt.so")
+    if verbose:
+        sys.stderr.write(r.stderr)
+    return out
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--fmad", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(a.fmad, verbose=a.verbose))

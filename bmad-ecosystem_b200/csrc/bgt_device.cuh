@@ -1,0 +1,441 @@
+// bgt_device.cuh -- FP64 element maps for one particle held in registers.
+//
+// Each function restates a reference routine (cited) for forward tracking
+// (direction = time_dir = orientation = +1) with the tracking species equal
+// to the reference species (charge_dir = rel_tracking_charge = 1).  The order
+// of floating-point operations follows the reference expressions; element
+// constants come pre-folded from the table (see bgt_table.h).
+#pragma once
+#include <stdint.h>
+
+#include "bgt_table.h"
+
+namespace bgt {
+
+constexpr double C_LIGHT = 2.99792458e8;                    // physical_constants.f90:34
+constexpr double PI_D = 3.141592653589793238462643383279;   // physical_constants.f90:12
+constexpr double TWOPI_D = 2 * PI_D;
+
+enum State : int32_t { ALIVE = 1, LOST = 2, LOST_NEG_X = 3, LOST_POS_X = 4, LOST_NEG_Y = 5, LOST_POS_Y = 6,
+                       LOST_PZ = 8 };
+
+// Per-launch constants.
+struct Glob {
+  double mc2;       // mass_of(species)
+  double mc2sq;     // mc2**2
+  double p0c;       // reference momentum (all elements share it)
+  double mal;       // bmad_com%max_aperture_limit
+  int32_t ap_on;    // bmad_com%aperture_limit_on
+  int32_t charge;
+};
+
+struct Part {
+  double x, px, y, py, z, pz, beta;
+  int32_t state;
+};
+
+// Per-particle memo of the drift's pz-only term (track_a_drift.f90:69,
+// first sqrt_one).  Value-identical: recomputed whenever pz differs.
+struct DriftMemo {
+  double pz;
+  double a;
+};
+
+__device__ __forceinline__ double sq(double x) { return x * x; }
+
+// sim_utils/special_functions/sqrt_one.f90:18-40
+__device__ __forceinline__ double sqrt_one(double x) {
+  double s = sqrt(1.0 + x);
+  double rad = s + 1.0;
+  return x / rad;
+}
+
+// sim_utils/special_functions/sinc.f90:15-45
+__device__ __forceinline__ double sinc_d(double x) {
+  if (fabs(x) < 1e-8) return 1.0;
+  return sin(x) / x;
+}
+
+// x**m as gfortran evaluates it (libgcc __powidf2 order of multiplies).
+__device__ __forceinline__ double powi_d(double x, int m) {
+  unsigned n = (unsigned)m;
+  double y = (n & 1u) ? x : 1.0;
+  while (n >>= 1) {
+    x = x * x;
+    if (n & 1u) y = y * x;
+  }
+  return y;
+}
+
+// bmad/low_level/mexp.f90:14-33 (m >= 0 here)
+__device__ __forceinline__ double mexp_d(double x, int m) { return m == 0 ? 1.0 : powi_d(x, m); }
+
+// c_multi(n, m, .true.) table (bmad/low_level/c_multi.f90:19-75), host-built.
+__constant__ double c_cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
+// c_multi(n, m) without the n! factor (the cc table of multipole_kick,
+// multipole_mod.f90:262-266).
+__constant__ double c_cm0[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
+
+// ---------------------------------------------------------------------------
+// Apertures
+
+// bmad/low_level/orbit_too_large.f90:26-120
+__device__ __forceinline__ bool orbit_too_large(Part& p, const Glob& G) {
+  if (p.x > G.mal) {
+    p.state = LOST_POS_X;
+    return true;
+  } else if (-p.x > G.mal) {
+    p.state = LOST_NEG_X;
+    return true;
+  }
+  if (p.y > G.mal) {
+    p.state = LOST_POS_Y;
+    return true;
+  } else if (-p.y > G.mal) {
+    p.state = LOST_NEG_Y;
+    return true;
+  }
+  double rel_p = 1 + p.pz;
+  if (rel_p < 0) {
+    p.state = LOST_PZ;
+    return true;
+  }
+  double f_unstable = p.px * p.px + p.py * p.py - rel_p * rel_p;
+  if (f_unstable > 0) {
+    if (fabs(p.px) > fabs(p.py)) {
+      p.state = p.px > 0 ? LOST_POS_X : LOST_NEG_X;
+    } else {
+      p.state = p.py > 0 ? LOST_POS_Y : LOST_NEG_Y;
+    }
+    return true;
+  }
+  return false;
+}
+
+// bmad/low_level/check_aperture_limit.f90:240-309 (lab-frame elliptical and
+// rectangular limits; the leading orbit_too_large is done by the caller).
+__device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32_t flags) {
+  if (flags & F_AP_ELLIPTICAL) {
+    double xp = p.x - ap[AP_XC];
+    double yp = p.y - ap[AP_YC];
+    double r = sq(xp / ap[AP_XW]) + sq(yp / ap[AP_YW]);
+    if (r < 1) return;
+    if (fabs(xp / ap[AP_XW]) > fabs(yp / ap[AP_YW])) {
+      p.state = xp > 0 ? LOST_POS_X : LOST_NEG_X;
+    } else {
+      p.state = yp > 0 ? LOST_POS_Y : LOST_NEG_Y;
+    }
+  } else {
+    double uf = 0, f;
+    const double x1 = ap[AP_X1], x2 = ap[AP_X2], y1 = ap[AP_Y1], y2 = ap[AP_Y2];
+    if (x1 != 0 && p.x < x1) {
+      f = fabs((p.x - x1) / (x2 - x1));
+      if (f > uf) {
+        p.state = LOST_NEG_X;
+        uf = f;
+      }
+    }
+    if (x2 != 0 && p.x > x2) {
+      f = fabs((p.x - x2) / (x2 - x1));
+      if (f > uf) {
+        p.state = LOST_POS_X;
+        uf = f;
+      }
+    }
+    if (y1 != 0 && p.y < y1) {
+      f = fabs((p.y - y1) / (y2 - y1));
+      if (f > uf) {
+        p.state = LOST_NEG_Y;
+        uf = f;
+      }
+    }
+    if (y2 != 0 && p.y > y2) {
+      f = fabs((p.y - y2) / (y2 - y1));
+      if (f > uf) {
+        p.state = LOST_POS_Y;
+        uf = f;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Drift: bmad/low_level/track_a_drift.f90:25-116
+
+__device__ __forceinline__ double drift_pz_term(const Part& p, const Glob& G, DriftMemo& m) {
+  if (p.pz != m.pz) {
+    double delta = p.pz;
+    double rel_pc = 1 + delta;
+    m.a = sqrt_one((G.mc2sq * (2 * delta + delta * delta)) / (sq(G.p0c * rel_pc) + G.mc2sq));
+    m.pz = p.pz;
+  }
+  return m.a;
+}
+
+template <bool REF_MOTION>
+__device__ __forceinline__ void track_a_drift(Part& p, double length, const Glob& G, DriftMemo& m) {
+  if (length == 0) return;
+  double rel_pc = 1 + p.pz;
+  double px_rel = p.px / rel_pc;
+  double py_rel = p.py / rel_pc;
+  double pxy2 = px_rel * px_rel + py_rel * py_rel;
+  if (pxy2 >= 1) {
+    p.state = LOST_PZ;
+    return;
+  }
+  double ps_rel = sqrt(1 - pxy2);
+  p.x = p.x + length * px_rel / ps_rel;
+  p.y = p.y + length * py_rel / ps_rel;
+  double dz;
+  if (p.beta > 0) {
+    if (REF_MOTION) {
+      double a = drift_pz_term(p, G, m);
+      dz = length * (a + sqrt_one(-pxy2) / ps_rel);
+    } else {
+      dz = -length / ps_rel;
+    }
+  } else {
+    if (REF_MOTION) {
+      dz = length * (1 - 1 / ps_rel);
+    } else {
+      dz = -length / ps_rel;
+    }
+  }
+  p.z = p.z + dz;
+}
+
+// bmad/code/tilt_coords.f90:18-53 with host-evaluated cos/sin of the angle
+__device__ __forceinline__ void tilt_coords(Part& p, double c, double s) {
+  double x = p.x, y = p.y, px = p.px, py = p.py;
+  p.x = c * x + s * y;
+  p.y = -s * x + c * y;
+  p.px = c * px + s * py;
+  p.py = -s * px + c * py;
+}
+
+// offset_particle set/unset for non-bend elements, bmad/code/offset_particle.f90
+// :183-334 (set) and :339-492 (unset), forward tracking.  Block layout in
+// bgt_table.h (MIS_*).
+__device__ __forceinline__ void matvec3(const double* w, double r0, double r1, double r2, double& o0, double& o1,
+                                        double& o2) {
+  o0 = w[0] * r0 + w[1] * r1 + w[2] * r2;
+  o1 = w[3] * r0 + w[4] * r1 + w[5] * r2;
+  o2 = w[6] * r0 + w[7] * r1 + w[8] * r2;
+}
+
+__device__ __forceinline__ void offset_set(Part& p, const double* mis, int32_t flags, const Glob& G, DriftMemo& m,
+                                           bool set_tilt) {
+  if (flags & F_OFFSET) {
+    double rel_p = 1 + p.pz;
+    if (flags & F_PITCH) {
+      double r0 = p.x - mis[MIS_XOFF], r1 = p.y - mis[MIS_YOFF], r2 = mis[MIS_R3SET];
+      double o0, o1, o2;
+      matvec3(mis + MIS_WINV, r0, r1, r2, o0, o1, o2);
+      o2 = o2 + mis[MIS_LHALF];
+      double s_body = o2;
+      double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+      if (pz <= 0) {
+        p.state = LOST_PZ;
+      } else {
+        double q0, q1, q2;
+        matvec3(mis + MIS_WINV, p.px, p.py, 1 * sqrt(pz), q0, q1, q2);
+        p.px = q0;
+        p.py = q1;
+        p.x = o0;
+        p.y = o1;
+      }
+      double ds = 0.0 - s_body;
+      if (fabs(ds) > 1e-14 && p.state == ALIVE) track_a_drift<false>(p, ds, G, m);
+    } else {
+      double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+      if (pz <= 0) {
+        p.state = LOST_PZ;
+      } else {
+        p.x = p.x - mis[MIS_XOFF];
+        p.y = p.y - mis[MIS_YOFF];
+      }
+      double ds = mis[MIS_DS_SET];
+      if (fabs(ds) > 1e-14 && p.state == ALIVE) track_a_drift<false>(p, ds, G, m);
+    }
+  }
+  if (flags & F_HV_KICK) {
+    p.px = p.px + mis[MIS_HK];
+    p.py = p.py + mis[MIS_VK];
+  }
+  if (set_tilt && (flags & F_TILT)) tilt_coords(p, mis[MIS_COS], mis[MIS_SIN]);
+}
+
+__device__ __forceinline__ void offset_unset(Part& p, const double* mis, int32_t flags, const Glob& G, DriftMemo& m,
+                                             bool set_tilt) {
+  if (set_tilt && (flags & F_TILT)) tilt_coords(p, mis[MIS_COSU], mis[MIS_SINU]);
+  if (flags & F_HV_KICK) {
+    p.px = p.px + mis[MIS_HK];
+    p.py = p.py + mis[MIS_VK];
+  }
+  if (flags & F_OFFSET) {
+    double rel_p = 1 + p.pz;
+    if (flags & F_PITCH) {
+      double o0, o1, o2;
+      matvec3(mis + MIS_W, p.x, p.y, mis[MIS_R3UNSET], o0, o1, o2);
+      o0 = o0 + mis[MIS_XOFF];
+      o1 = o1 + mis[MIS_YOFF];
+      o2 = o2 + mis[MIS_ZADD];
+      double s_lab = o2;
+      double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+      if (pz <= 0) {
+        p.state = LOST_PZ;
+      } else {
+        double q0, q1, q2;
+        matvec3(mis + MIS_W, p.px, p.py, 1 * sqrt(pz), q0, q1, q2);
+        p.px = q0;
+        p.py = q1;
+        p.x = o0;
+        p.y = o1;
+      }
+      double ds = 2 * mis[MIS_LHALF] - s_lab;
+      if (fabs(ds) > 1e-14 && p.state == ALIVE) track_a_drift<false>(p, ds, G, m);
+    } else {
+      double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+      if (pz <= 0) {
+        p.state = LOST_PZ;
+      } else {
+        p.x = p.x + mis[MIS_XOFF];
+        p.y = p.y + mis[MIS_YOFF];
+      }
+      double ds = mis[MIS_DS_UNSET];
+      if (fabs(ds) > 1e-14 && p.state == ALIVE) track_a_drift<false>(p, ds, G, m);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multipole kicks: bmad/modules/multipole_mod.f90:82-174 (ab_multipole_kicks,
+// magnetic) and :314-401 (ab_multipole_kick).  The factor
+// r = ele%value(p0c)/orbit%p0c and the charge/orientation factor are exactly
+// 1.0 here, so a2 = scale * a, b2 = scale * b.
+__device__ __forceinline__ void ab_multipole_kicks(Part& p, const double* an, const double* bn, int ix_max,
+                                                   double scale) {
+  double kx_tot = 0, ky_tot = 0;
+  const double x = p.x, y = p.y;
+  for (int n = 0; n <= ix_max; n++) {
+    double a = an[n], b = bn[n];
+    double kx = 0, ky = 0;
+    if (!(a == 0 && b == 0)) {
+      double a2 = scale * a, b2 = scale * b;
+      for (int m = 0; m <= n; m += 2) {
+        double f = c_cm[n][m] * mexp_d(x, n - m) * mexp_d(y, m);
+        kx = kx + b2 * f;
+        ky = ky - a2 * f;
+      }
+      for (int m = 1; m <= n; m += 2) {
+        double f = c_cm[n][m] * mexp_d(x, n - m) * mexp_d(y, m);
+        kx = kx + a2 * f;
+        ky = ky + b2 * f;
+      }
+    }
+    kx_tot = kx_tot + kx;
+    ky_tot = ky_tot + ky;
+  }
+  p.px = p.px + kx_tot;
+  p.py = p.py + ky_tot;
+}
+
+// ---------------------------------------------------------------------------
+// Quadrupole body helpers
+
+// bmad/low_level/quad_mat2_calc.f90:22-81 (mat2 and z_coef)
+struct QMat {
+  double cx, m01, m10, z0, z1, z2;
+};
+
+__device__ __forceinline__ QMat quad_mat2_calc(double k1, double length, double rel_p) {
+  QMat q;
+  double sqrt_k = sqrt(fabs(k1));
+  double sk_l = sqrt_k * length;
+  double cx, sx;
+  if (fabs(sk_l) < 1e-10) {
+    double k_l2 = k1 * (length * length);
+    cx = 1 + k_l2 / 2;
+    sx = (1 + k_l2 / 6) * length;
+  } else if (k1 < 0) {
+    double s, c;
+    sincos(sk_l, &s, &c);
+    cx = c;
+    sx = s / sqrt_k;
+  } else {
+    cx = cosh(sk_l);
+    sx = sinh(sk_l) / sqrt_k;
+  }
+  q.cx = cx;
+  q.m01 = sx / rel_p;
+  q.m10 = k1 * sx * rel_p;
+  q.z0 = k1 * (-cx * sx + length) / 4;
+  q.z1 = -k1 * (sx * sx) / (2 * rel_p);
+  q.z2 = -(cx * sx + length) / (4 * (rel_p * rel_p));
+  return q;
+}
+
+// bmad/low_level/low_energy_z_correction.f90:22-58; lez = LEZ block
+__device__ __forceinline__ double low_energy_z_correction(const Part& p, const double* lez, double ds) {
+  double beta0 = lez[LEZ_BETA0];
+  double pz = p.pz;
+  if (lez[LEZ_MASS] * ((beta0 * pz) * (beta0 * pz)) < lez[LEZ_3E7]) {
+    return ds * pz * (1 - 3 * (pz * (beta0 * beta0)) / 2 + (pz * pz) * lez[LEZ_F]) * lez[LEZ_ME2];
+  }
+  return ds * (p.beta - beta0) / beta0;
+}
+
+// bmad/low_level/apply_energy_kick.f90:23-74
+__device__ __forceinline__ void apply_energy_kick(Part& p, double dE, const Glob& G) {
+  double pc = (1 + p.pz) * G.p0c;
+  double beta_old = p.beta;
+  double E_old = pc / p.beta;
+  double E_new = E_old + dE;
+  if (E_new < G.mc2) {
+    p.pz = -1;
+    p.beta = 0;
+    p.state = LOST_PZ;
+    return;
+  }
+  p.pz = p.pz + (1 + p.pz) * sqrt_one((2 * E_old * dE + dE * dE) / (pc * pc));
+  double pc_new = G.p0c * (1 + p.pz);
+  double beta_new = pc_new / E_new;
+  p.z = p.z * beta_new / beta_old;
+  p.beta = beta_new;
+}
+
+// ---------------------------------------------------------------------------
+// Hwang hard-edge bend fringe, bmad/modules/fringe_mod.f90:240-418 (td = +1)
+template <bool ENTERING>
+__device__ __forceinline__ void hwang_edge(Part& p, const double* E) {
+  const double gt = E[EDGE_GT], gt2 = E[EDGE_GT2], gs2 = E[EDGE_GS2], k1_tane = E[EDGE_K1TANE];
+  const double fg = E[EDGE_FG];
+  double e_factor = 1 / (1 + p.pz);
+  double v0 = p.x, v1 = p.px, v2 = p.y, v3 = p.py, v4 = p.z;
+  double dx, dpx, dy, dpy, dz;
+  if (ENTERING) {
+    dx = (-gt2 * (v0 * v0) + gs2 * (v2 * v2)) * e_factor / 2;
+    dpx = (E[EDGE_C1] * (v2 * v2) / 2 + gt2 * (v0 * v1 - v2 * v3) + k1_tane * (v0 * v0 - v2 * v2)) * e_factor;
+    dy = gt2 * v0 * v2 * e_factor;
+    dpy = (fg * v2 - gt2 * v0 * v3 - E[EDGE_GPG] * v1 * v2 - E[EDGE_K1TANE2] * v0 * v2) * e_factor;
+    dz = (e_factor * e_factor) * 0.5 *
+         ((v2 * v2) * fg + (v0 * v0 * v0) * E[EDGE_C3] / 6.0 + 0.5 * v0 * (v2 * v2) * E[EDGE_C4] +
+          ((v0 * v0) * v1 - 2.0 * v0 * v2 * v3) * gt2 - v1 * (v2 * v2) * gs2);
+  } else {
+    dx = (gt2 * (v0 * v0) - gs2 * (v2 * v2)) * e_factor / 2;
+    dpx = (gt2 * (v2 * v3 - v0 * v1) + k1_tane * (v0 * v0 - v2 * v2) - E[EDGE_C1] * (v0 * v0 + v2 * v2) / 2) *
+          e_factor;
+    dy = -gt2 * v0 * v2 * e_factor;
+    dpy = (fg * v2 + gt2 * v0 * v3 + E[EDGE_GPG] * v1 * v2 + E[EDGE_GTGS2_2K1] * v0 * v2) * e_factor;
+    dz = (e_factor * e_factor) * 0.5 *
+         ((v2 * v2) * fg + (v0 * v0 * v0) * E[EDGE_C3] / 6.0 + 0.5 * v0 * (v2 * v2) * E[EDGE_C4] -
+          ((v0 * v0) * v1 - 2.0 * v0 * v2 * v3) * gt2 + v1 * (v2 * v2) * gs2);
+  }
+  p.x = v0 + 1.0 * dx;
+  p.px = v1 + 1.0 * (dpx + gt * v0);
+  p.y = v2 + 1.0 * dy;
+  p.py = v3 + 1.0 * (dpy - gt * v2);
+  p.z = v4 + 1.0 * dz;
+}
+
+}  // namespace bgt

@@ -1,0 +1,136 @@
+// bgt_table.h -- device element table: one variable-length record per
+// lattice element, packed as doubles so the whole table of a ring (a few
+// tens of KB) is staged once per CTA into shared memory by a bulk TMA copy
+// and then read by broadcast from there for every turn.
+//
+// Record = 4-double header (8 x int32) + kind-specific FP64 parameters.
+// Every value that depends only on the element (never on the particle) is
+// computed on the host with the same operation order the reference uses
+// (e.g. sin/cos of tilts, Hwang edge coefficients, element-constant products
+// that sit leftmost in a reference expression), so device results are
+// value-identical to evaluating the reference expression in full.
+#pragma once
+#include <stdint.h>
+
+#define BGT_MAXPOLE_DEV 21  // highest multipole order (n_pole_maxx)
+
+namespace bgt {
+
+enum Kind : int32_t {
+  K_MARKER = 0,       // nothing but aperture checks
+  K_DRIFT = 1,        // track_a_drift
+  K_QUAD = 2,         // track_a_quadrupole
+  K_BEND = 3,         // track_a_bend (+ Hwang edges)
+  K_THICK_MULT = 4,   // track_a_thick_multipole (sext, oct, thick_multipole, kickers, collimators ...)
+  K_THIN_MULT = 5,    // multipole / ab_multipole (track1_bmad.f90:142-166)
+  K_RFCAVITY = 6,     // track_a_rfcavity
+};
+
+enum Flag : int32_t {
+  F_OFFSET = 1 << 0,      // x/y/z offset or pitch -> offset_particle translation
+  F_PITCH = 1 << 1,       // x/y pitch -> W rotation and drift to the edge
+  F_TILT = 1 << 2,        // tilt_coords with tilt_tot (or ref_tilt for bends)
+  F_AP_ENTRANCE = 1 << 3, // aperture checked at the entrance edge
+  F_AP_EXIT = 1 << 4,     // aperture checked at the exit edge
+  F_AP_ELLIPTICAL = 1 << 5,
+  F_AP_RECT = 1 << 6,
+  F_HV_KICK = 1 << 7,      // offset_particle set_hv1 kicks (rfcavity only)
+  F_EDGE_IN = 1 << 8,      // Hwang edge at entrance
+  F_EDGE_OUT = 1 << 9,     // Hwang edge at exit
+  F_MISALIGN = 1 << 10,    // has_misalign (offset_particle is called)
+  F_SEMI_LINEAR_OK = 1 << 11, // bend: dg == 0 so the near-axis semi-linear map may apply
+  F_K1_BODY = 1 << 12,     // bend: sbend_body_with_k1_map
+  F_DRIFT_BODY = 1 << 13,  // bend: body is a plain drift (g == dg == 0 or step_len == 0)
+  F_IS_OFF = 1 << 14,      // bend is off (is_on = F)
+};
+
+struct RecHdr {
+  int32_t kind;
+  int32_t ix_ele;
+  int32_t size_dw;    // record size in doubles, header included
+  int32_t flags;
+  int32_t n_step;     // body steps (quad, bend, thick multipole), slices (rf)
+  int32_t ix_mag_max; // highest multipole order with a kick (-1 = none)
+  int32_t aux0;       // kind-specific
+  int32_t aux1;       // kind-specific
+};
+static_assert(sizeof(RecHdr) == 32, "header is 4 doubles");
+
+constexpr int HDR_DW = 4;
+
+// ---- parameter offsets (in doubles, relative to the record start) ----
+// Common blocks appear in this order after the header when their flag is set:
+//   misalignment block (F_MISALIGN):      MIS_N doubles
+//   aperture block (F_AP_*):              AP_N doubles
+// then the kind block.
+constexpr int MIS_XOFF = 0, MIS_YOFF = 1, MIS_ZOFF = 2, MIS_LHALF = 3, MIS_COS = 4, MIS_SIN = 5;
+constexpr int MIS_WINV = 6;   // 9 doubles: w_mat_inv (set), row-major
+constexpr int MIS_W = 15;     // 9 doubles: w_mat (unset), row-major
+constexpr int MIS_HK = 24, MIS_VK = 25;  // 0.5*charge_dir*hkick, 0.5*charge_dir*vkick
+constexpr int MIS_DS_SET = 26;    // drift length to the body edge after the set translation (no pitch)
+constexpr int MIS_DS_UNSET = 27;  // drift length back to the lab edge after unset (no pitch)
+constexpr int MIS_R3SET = 28;     // 0 - (z_offset + ds_center) on set
+constexpr int MIS_R3UNSET = 29;   // 0 - ds_center on unset
+constexpr int MIS_ZADD = 30;      // z_offset + L/2 on unset
+constexpr int MIS_COSU = 31, MIS_SINU = 32;  // cos/sin of -tilt (unset)
+constexpr int MIS_N = 33;
+
+constexpr int AP_X1 = 0, AP_X2 = 1, AP_Y1 = 2, AP_Y2 = 3;  // x1_lim = -x1_limit, ...
+constexpr int AP_XW = 4, AP_XC = 5, AP_YW = 6, AP_YC = 7;  // elliptical width2/center
+constexpr int AP_N = 8;
+
+// Drift: L
+constexpr int DR_L = 0, DR_N = 1;
+
+// Quadrupole
+constexpr int Q_LEN = 0;      // length (time_dir * L)
+constexpr int Q_B1 = 1;       // charge_dir * b1
+constexpr int Q_STEP = 2;     // step_len
+constexpr int Q_RHALF = 3;    // r_step / 2
+constexpr int Q_RSTEP = 4;    // r_step
+constexpr int Q_LEZ = 5;      // low_energy_z_correction constants, LEZ_N doubles
+constexpr int Q_N = Q_LEZ + 6;
+constexpr int LEZ_BETA0 = 0, LEZ_MB2_THRESH = 1, LEZ_F = 2, LEZ_ME2 = 3, LEZ_MASS = 4, LEZ_3E7 = 5;
+
+// Thick multipole: step_len, r_step/2, r_step
+constexpr int TM_STEP = 0, TM_RHALF = 1, TM_RSTEP = 2, TM_N = 3;
+
+// Bend
+constexpr int B_LEN = 0, B_G = 1, B_DG = 2, B_GTOT = 3, B_STEP = 4, B_ANGLE = 5, B_RSTEP = 6;
+constexpr int B_COSA = 7, B_SINA = 8, B_SINCA = 9, B_COSCA = 10, B_BETAREF = 11, B_B1 = 12;
+constexpr int B_LL2GCOSC = 13;    // ((step_len*step_len)*g)*cosc_a      (exact body)
+constexpr int B_LLSINC = 14;      // step_len*sinc_a                     (exact body, semi-linear)
+constexpr int B_M56C = 15;        // (g*ll)**2 * sincc(angle)            (semi-linear)
+constexpr int B_GLLSINC = 16;     // (g*ll)*sinc_a                       (semi-linear)
+constexpr int B_GLL2COSC = 17;    // (g*ll**2)*cosc_a                    (semi-linear)
+constexpr int B_GSIN = 18;        // g*sin_a                             (semi-linear)
+constexpr int B_FP0C = 19;        // multipole kick: r_step * p0c / (c_light * charge)
+constexpr int B_CDIR = 20;        // c_dir = charge (multipole kick)
+constexpr int B_LEZ = 21;         // low_energy_z_correction block (k1 body)
+constexpr int B_K1 = B_LEZ + 6;   // k1 body: k1 = b1/L, length (= L/n_step), g_tot
+constexpr int B_EDGE = B_K1 + 3;  // Hwang edge constants, entrance block then exit block
+// Hwang edge block (fringe_mod.f90:240-418); C1 is (gt*g_tot)*(1+2*tan_e**2)
+// at the entrance and gt*gt2 at the exit, the leftmost constant factors of
+// the dpx terms.
+constexpr int EDGE_GT = 0, EDGE_GT2 = 1, EDGE_GS2 = 2, EDGE_K1TANE = 3, EDGE_K1TANE2 = 4, EDGE_FG = 5,
+              EDGE_C1 = 6, EDGE_C3 = 7, EDGE_C4 = 8, EDGE_GPG = 9, EDGE_GTGS2_2K1 = 10;
+constexpr int EDGE_N = 11;
+constexpr int B_N = B_EDGE + 2 * EDGE_N;
+
+// Thin multipole: per pole n (0..ix_mag_max): knl, cos(tilt), sin(tilt), tilt_is_zero
+constexpr int TH_REFORB = 0;  // ref_orb_offset (1.0 for multipole$, else 0)
+constexpr int TH_N = 1;
+constexpr int TH_POLE = 4;    // doubles per pole
+
+// RF cavity
+constexpr int RF_LEN = 0, RF_VOLT = 1, RF_PHI0 = 2, RF_FREQ = 3, RF_NSLICE = 4, RF_SLICE_L = 5;
+constexpr int RF_TWOPI_F = 6;  // twopi * rf_frequency
+constexpr int RF_HALF_AMP_HI = 7, RF_HALF_AMP_LO = 8;  // 0.5/f as double-double
+constexpr int RF_PHI0_MP = 9;  // twopi * phi0_multipass
+constexpr int RF_RHALF = 10;   // 0.5 * r_step (multipole kicks)
+constexpr int RF_N = 11;
+
+// Multipole arrays for quad / bend / thick multipole / rf follow the kind
+// block: an[0..ix_mag_max], bn[0..ix_mag_max].
+
+}  // namespace bgt

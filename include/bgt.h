@@ -1,0 +1,222 @@
+/*
+ * bgt.h -- C ABI of libbgt, the B200 FP64 multi-particle tracker for Bmad
+ * `bmad_standard` lattices.
+ *
+ * The entry points replace, for the tracking methods and element types listed
+ * below, the reference's multi-particle tracking call surface:
+ *
+ *   bgt_track_turns   <- the turn loop of long_term_tracking in BEAM mode,
+ *                        bsim/modules/lt_tracking_mod.f90:1631-1695, i.e.
+ *                        ltt_track_bmad_bunch (:3186-3225) -> track_bunch
+ *                        (bmad/multiparticle/beam_mod.f90:103-170) ->
+ *                        track1_bunch_hom (beam_utils.f90:32-160) ->
+ *                        track1 (bmad/code/track1.f90:43) per particle per
+ *                        element.  Installed through track1_bunch_hook_ptr
+ *                        (bmad/modules/bmad_routine_interface.f90:3927-3936)
+ *                        or as a 'GPU' case of lttp%tracking_method
+ *                        (lt_tracking_mod.f90:1636-1670).
+ *   bgt_track_elements <- track_all / track_many over a contiguous range of
+ *                        elements (bmad/code/track_all.f90:25,
+ *                        bmad/code/track_many.f90:50), and, with a range of
+ *                        one element, track1 (bmad/code/track1.f90:43).
+ *   bgt_da_scan_grid  <- dynamic_aperture_scan / dynamic_aperture_point
+ *                        (bmad/modules/dynamic_aperture_mod.f90:27,284) with
+ *                        the bisection replaced by a polar amplitude grid.
+ *
+ * Conventions (kept from the reference so the shim is a pass-through):
+ *  - Element keys, fringe_type, fringe_at/aperture_at and aperture_type use
+ *    Bmad's integer codes (bmad/modules/bmad_struct.f90:157-168,372,1681-1695).
+ *  - Particle state codes are Bmad's coord_struct%state codes
+ *    (bmad_struct.f90:522-527): alive = 1, lost = 2, lost_neg_x = 3,
+ *    lost_pos_x = 4, lost_neg_y = 5, lost_pos_y = 6, lost_pz = 8.
+ *    A lost particle is a state, not an error (track1.f90:38-40).
+ *  - Coordinates are Bmad phase-space coordinates (x, px, y, py, z, pz),
+ *    stored structure-of-arrays: vec6[c * n + i] is coordinate c of particle i.
+ *  - ix_ele_lost is the lost-at element's ix_ele (the `track_state` of
+ *    track_all, track_all.f90:17-18); ix_turn_lost is the 0-based turn index in
+ *    which the particle was lost (bunch%ix_turn before that turn,
+ *    lt_tracking_mod.f90:1633).  Both stay -1 for particles that survive.
+ *  - Every function returns 0 on success or a negative BGT_E* code; the
+ *    message is available from bgt_last_error().  Nothing aborts.
+ *  - Host buffers are caller-owned; device buffers are owned by the handle or
+ *    by the caller (the *_device entry points).
+ *
+ * Scope: forward tracking (direction = time_dir = orientation = +1), relative
+ * RF time (bmad_com%absolute_time_tracking = F), magnetic multipoles, no
+ * radiation/spin.  bgt_create rejects any element outside that scope with
+ * BGT_EUNSUPPORTED and names the element.
+ */
+#ifndef BGT_H
+#define BGT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BGT_N_POLE 22 /* n_pole_maxx + 1, bmad_struct.f90:48 */
+
+/* Bmad element keys (bmad_struct.f90:1681-1695). */
+enum {
+  BGT_DRIFT = 1,
+  BGT_SBEND = 2,
+  BGT_QUADRUPOLE = 3,
+  BGT_SEXTUPOLE = 5,
+  BGT_RFCAVITY = 9,
+  BGT_MARKER = 14,
+  BGT_KICKER = 15,
+  BGT_OCTUPOLE = 17,
+  BGT_MULTIPOLE = 19,
+  BGT_AB_MULTIPOLE = 22,
+  BGT_MONITOR = 31,
+  BGT_INSTRUMENT = 32,
+  BGT_HKICKER = 33,
+  BGT_VKICKER = 34,
+  BGT_RCOLLIMATOR = 35,
+  BGT_ECOLLIMATOR = 36,
+  BGT_PIPE = 44,
+  BGT_THICK_MULTIPOLE = 67
+};
+
+/* fringe_type (bmad_struct.f90:164-168); 1 = none$ */
+enum { BGT_FRINGE_NONE = 1, BGT_FRINGE_SOFT_EDGE_ONLY = 2, BGT_FRINGE_HARD_EDGE_ONLY = 3,
+       BGT_FRINGE_FULL = 4, BGT_FRINGE_BASIC_BEND = 7 };
+/* fringe_at / aperture_at (bmad_struct.f90:372) */
+enum { BGT_ENTRANCE_END = 1, BGT_EXIT_END = 2, BGT_BOTH_ENDS = 3, BGT_NO_END = 4 };
+/* aperture_type (bmad_struct.f90:157); 0 = no aperture limits set */
+enum { BGT_APERTURE_NONE = 0, BGT_APERTURE_RECTANGULAR = 2, BGT_APERTURE_ELLIPTICAL = 3 };
+
+/* coord_struct%state (bmad_struct.f90:522-527) */
+enum { BGT_ALIVE = 1, BGT_LOST = 2, BGT_LOST_NEG_X = 3, BGT_LOST_POS_X = 4, BGT_LOST_NEG_Y = 5,
+       BGT_LOST_POS_Y = 6, BGT_LOST_PZ = 8 };
+
+/* error codes */
+enum { BGT_OK = 0, BGT_EINVAL = -1, BGT_EUNSUPPORTED = -2, BGT_ECUDA = -3, BGT_ENOMEM = -4,
+       BGT_ETIMEOUT = -5, BGT_ETOOLARGE = -6 };
+
+/*
+ * One lattice element, i.e. the ele_struct fields the bmad_standard path
+ * reads (ele%value(...) entries by name, bmad_struct.f90:1762-1879).
+ * an/bn and an_elec/bn_elec are what
+ *   multipole_ele_to_ab(ele, .false., ix, an, bn, magnetic$, include_kicks$)
+ *   multipole_ele_to_ab(ele, .false., ix, an_elec, bn_elec, electric$)
+ * return (bmad/code/multipole_ele_to_ab.f90:31) -- b1 NOT pulled out; the
+ * library pulls it where track_a_quadrupole / track_a_bend do.  knl/tn are
+ * multipole_ele_to_kt(ele, .true., ix, knl, tn) (multipole_ele_to_kt.f90:29),
+ * used by multipole and ab_multipole elements.
+ */
+typedef struct bgt_element {
+  int32_t key;
+  int32_t ix_ele;
+  int32_t is_on;
+  int32_t num_steps;
+  int32_t fringe_type;
+  int32_t fringe_at;
+  int32_t aperture_type;
+  int32_t aperture_at;
+  int32_t offset_moves_aperture;
+  int32_t exact_multipoles; /* 0 = off$ */
+  int32_t has_misalign;     /* ele%bookkeeping_state%has_misalign */
+  int32_t reserved;
+  double l, k1, k2, k3, g, dg, e1, e2, fint, hgap, fintx, hgapx;
+  double voltage, phi0, phi0_multipass, rf_frequency, coupler_strength;
+  double p0c, e_tot, ds_step;
+  double x_offset, y_offset, z_offset, x_pitch, y_pitch, tilt, ref_tilt, roll;
+  double hkick, vkick, kick;
+  double x1_limit, x2_limit, y1_limit, y2_limit;
+  double an[BGT_N_POLE], bn[BGT_N_POLE];
+  double an_elec[BGT_N_POLE], bn_elec[BGT_N_POLE];
+  double knl[BGT_N_POLE], tn[BGT_N_POLE];
+} bgt_element;
+
+/* Tracked species (lat%param%particle) and bmad_com switches. */
+typedef struct bgt_species {
+  double mass;               /* mass_of(species) [eV] */
+  int32_t charge;            /* charge_of(species) [e] */
+  int32_t aperture_limit_on; /* bmad_com%aperture_limit_on (default 1) */
+  double max_aperture_limit; /* bmad_com%max_aperture_limit (default 1e3 m) */
+} bgt_species;
+
+/* Launch tiles chosen by the autotuner (0 = let the library choose). */
+typedef struct bgt_tuning {
+  int32_t threads_per_block; /* particles per CTA */
+  int32_t blocks_per_sm;     /* resident CTAs per SM for the persistent grid */
+  int32_t turns_per_launch;  /* turns per persistent-kernel launch (graph node) */
+  int32_t compact_every;     /* compact lost particles every this many turns (0 = never) */
+} bgt_tuning;
+
+typedef struct bgt_handle bgt_handle;
+
+/*
+ * Flattens n_variants lattices of n_ele elements each (eles[v * n_ele + e])
+ * into the device element tables (structure-of-records, one table per
+ * variant).  Each variant is a copy of the same ring with its own element
+ * values (error seeds, sextupole settings).  `device` is the CUDA ordinal.
+ */
+int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t n_variants,
+               const bgt_species* species, int32_t device);
+int bgt_destroy(bgt_handle* h);
+const char* bgt_last_error(const bgt_handle* h);
+
+/* Table bytes per variant and the tuning currently in use. */
+int bgt_table_info(const bgt_handle* h, int64_t* table_bytes, int32_t* n_records);
+int bgt_set_tuning(bgt_handle* h, const bgt_tuning* t);
+int bgt_get_tuning(const bgt_handle* h, bgt_tuning* t);
+
+/*
+ * Track n particles for n_turns turns starting at turn index turn0, in place.
+ * HOST buffers (the long_term_tracking drop-in): vec6[6*n], beta[n] (FP64),
+ * state/ix_ele_lost/ix_turn_lost[n] (int32).  variant[n] selects each
+ * particle's lattice variant (NULL = variant 0).  Particles whose state is
+ * not alive are left untouched.  Copies in, tracks, copies out.
+ */
+int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+                    int32_t* ix_turn_lost, const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns);
+
+/*
+ * Same, DEVICE buffers already resident in HBM, enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).  Asynchronous.
+ * Uses library-owned scratch sized on first use (grown as needed).
+ */
+int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state,
+                           int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n,
+                           int32_t turn0, int32_t n_turns, void* stream);
+
+/*
+ * Track n particles through table elements [e_begin, e_end) of their variant
+ * once (no turn wrap), HOST buffers.  e_end - e_begin == 1 is track1
+ * (bmad/code/track1.f90:43) including its two check_aperture_limit calls.
+ */
+int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+                       const int32_t* variant, int64_t n, int32_t e_begin, int32_t e_end);
+
+/*
+ * Dynamic-aperture scan on a polar grid, one launch for all variants:
+ * for each variant v, angle a (n_angle in [angle_min, angle_max]), radius r
+ * (n_radius from 0 to r_max), and momentum offset d (n_delta values in
+ * deltas[]), the particle starts at ref_orbit[v] (6 coords, the closed orbit
+ * of variant v at the start, with pz set to deltas[d] ... plus eta*pz when
+ * the caller includes it) + (r cos a, 0, r sin a * y_scale, 0, 0, 0) and is
+ * tracked n_turns turns.  da_radius[((v * n_delta) + d) * n_angle + a] receives
+ * the largest grid radius below the first lost one along that ray (the
+ * lower bracket x0 of dynamic_aperture_point, dynamic_aperture_mod.f90:
+ * 335-388); survive_turns (optional, may be NULL) receives, per particle in
+ * (v, d, a, r) order, the turns survived (n_turns if never lost).
+ */
+int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_used, const double* deltas,
+                     int32_t n_delta, int32_t n_angle, double angle_min, double angle_max, int32_t n_radius,
+                     double r_max, double y_scale, int32_t n_turns, double* da_radius, int32_t* survive_turns);
+
+/* Number of this library's kernels launched since the handle was created. */
+int64_t bgt_kernel_launch_count(const bgt_handle* h);
+
+/* Measured FP64 FMA throughput of `device` in TFLOP/s (2 flops per FMA):
+ * the roofline denominator for the tracking kernel.  No reference
+ * counterpart (measurement helper). */
+int bgt_fp64_peak_tflops(int32_t device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

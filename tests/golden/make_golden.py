@@ -1,0 +1,59 @@
+"""Extract the reference's golden vectors for the bmad_standard path into
+tests/golden/*.json.  Reads the reference checkout (default /root/reference)
+as text; the JSON files are committed so tests never need the reference.
+
+    python tests/golden/make_golden.py [REFERENCE_ROOT]
+
+Sources (relative to the reference root):
+  regression_tests/tracking_method_test/output.correct  ("<ELE>: Bmad_Standard" rows)
+  regression_tests/fringe_test/output.correct           (Hwang edge kick deltas)
+  regression_tests/aperture_test/output.correct         (aperture states, unstable factors)
+"""
+import json
+import re
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+
+def parse_line(line):
+    m = re.match(r'\s*"([^"]+)"\s+(ABS|REL|STR|VEC_REL)\s+(\S+)\s+(.*)$', line)
+    if not m:
+        return None
+    name, kind, tol, rest = m.groups()
+    vals = rest.split()
+    return name, kind, float(tol) if kind != "STR" else tol, vals
+
+
+def main(ref: Path):
+    out = {}
+    tm = (ref / "regression_tests/tracking_method_test/output.correct").read_text().splitlines()
+    rows = {}
+    for line in tm:
+        p = parse_line(line)
+        if not p:
+            continue
+        name, kind, tol, vals = p
+        if not name.endswith(": Bmad_Standard") or "-" in name.split(":")[0]:
+            continue
+        rows[name.split(":")[0]] = {"tol": tol, "values": [float(v) for v in vals], "text": vals}
+    out["tracking_method"] = rows
+    fr = {}
+    for line in (ref / "regression_tests/fringe_test/output.correct").read_text().splitlines():
+        p = parse_line(line)
+        if p and p[0] in ("Up-Orb", "Dn-Orb"):
+            fr[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3]], "text": p[3]}
+    out["fringe"] = fr
+    ap = {}
+    for line in (ref / "regression_tests/aperture_test/output.correct").read_text().splitlines():
+        p = parse_line(line)
+        if p and re.match(r"(EC|RC)_[SU]_", p[0]):
+            ap[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3]], "text": p[3]}
+    out["aperture"] = ap
+    (HERE / "reference_golden.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+    print(f"tracking_method rows: {len(rows)}, fringe rows: {len(fr)}, aperture rows: {len(ap)}")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))

@@ -1,0 +1,107 @@
+"""Shared fixtures for parity tests: an element zoo, seeded particles, and
+the oracle / GPU runners compared by the tests."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from bgt import lattice as L
+from bgt import rings
+
+# Tolerances (FP64).  Per coordinate c, a GPU value g and oracle value o agree
+# when |g - o| <= RTOL * (|o| + rms_c), rms_c the bunch RMS of coordinate c:
+# relative to the value, with the coordinate's bunch scale as the floor for
+# values that pass near zero.
+RTOL_ONE_TURN = 1e-13
+RTOL_1000_TURNS = 1e-9
+
+
+def zoo_lattice(apertures: bool = True) -> L.Lattice:
+    """One of every element form the GPU supports, at the 5 GeV ring energy,
+    with misalignments, multipoles, edges and apertures."""
+    E = []
+    E.append(L.Element("drift", "D", {"l": 0.7}))
+    E.append(L.Element("quadrupole", "Q0", {"l": 0.4, "k1": 0.8}))
+    E.append(L.Element("quadrupole", "QERR", {"l": 0.4, "k1": -0.7, "x_offset": 2e-4, "y_offset": -1e-4,
+                                              "tilt": 3e-3, "r0_mag": 0.01},
+                       a_pole={3: 2e-4, 5: -1e-4}, b_pole={3: -3e-4, 4: 1e-4, 6: 2e-4}))
+    E.append(L.Element("quadrupole", "QPITCH", {"l": 0.5, "k1": 0.6, "x_pitch": 2e-4, "y_pitch": -3e-4,
+                                                "z_offset": 1e-3, "hkick": 1e-5}))
+    E.append(L.Element("quadrupole", "QZERO", {"l": 0.3, "k1": 0.0, "hkick": 2e-5}))
+    E.append(L.Element("sextupole", "S", {"l": 0.2, "k2": 25.0}))
+    E.append(L.Element("sextupole", "SERR", {"l": 0.2, "k2": -30.0, "x_offset": 1e-4, "tilt": -2e-3,
+                                             "r0_mag": 0.01}, a_pole={4: 1e-4}, b_pole={5: 2e-4}))
+    E.append(L.Element("octupole", "O", {"l": 0.3, "k3": 300.0, "tilt": 0.1}, num_steps=4))
+    E.append(L.Element("thick_multipole", "TM", {"l": 0.5, "x_offset": 1e-4}, a_pole={2: 1.0}, b_pole={3: 20.0}))
+    E.append(L.Element("sbend", "B", {"l": 2.0, "g": rings.ANGLE / 2.0}))
+    E.append(L.Element("sbend", "BE", {"l": 1.5, "g": 0.02, "e1": 0.05, "e2": -0.03, "fint": 0.5, "hgap": 0.02}))
+    E.append(L.Element("sbend", "BK1", {"l": 1.2, "g": 0.015, "k1": 0.2, "e1": 0.02, "e2": 0.01}))
+    E.append(L.Element("sbend", "BMUL", {"l": 1.0, "g": 0.03, "k2": 2.0, "ref_tilt": 0.05}, b_pole={4: 1e-3}))
+    E.append(L.Element("sbend", "BHARD", {"l": 1.0, "g": -0.01, "e1": 0.1, "e2": 0.1, "fint": 0.3, "hgap": 0.05},
+                       fringe_type="hard_edge_only"))
+    E.append(L.Element("multipole", "M", {"x_offset": 1e-4}, a_pole={1: 0.05, 3: 40.0}, b_pole={1: 0.2, 3: 0.7}))
+    E.append(L.Element("multipole", "M0", {}, a_pole={0: 1e-4, 2: 3.0}))
+    E.append(L.Element("ab_multipole", "AB", {"x_offset": 2e-4, "tilt": 0.1}, a_pole={2: 1.0}, b_pole={2: 2.0}))
+    E.append(L.Element("hkicker", "HK", {"l": 0.2, "kick": 1e-5}))
+    E.append(L.Element("vkicker", "VK", {"l": 0.2, "kick": -2e-5}))
+    E.append(L.Element("kicker", "K", {"l": 0.3, "hkick": 1e-5, "vkick": 2e-5}))
+    E.append(L.Element("monitor", "MON", {"l": 0.1}))
+    E.append(L.Element("instrument", "INS", {"l": 0.1, "x_offset": 1e-4}))
+    E.append(L.Element("rcollimator", "RC", {"l": 0.2, "x1_limit": 0.02, "x2_limit": 0.02, "y1_limit": 0.01,
+                                             "y2_limit": 0.012}))
+    E.append(L.Element("ecollimator", "EC", {"l": 0.2, "x1_limit": 0.015, "x2_limit": 0.02, "y1_limit": 0.01,
+                                             "y2_limit": 0.01}))
+    E.append(L.Element("rfcavity", "RF", {"l": 0.5, "voltage": 5e6, "phi0": 0.02, "rf_frequency": 499.98e6}))
+    E.append(L.Element("rfcavity", "RFMIS", {"l": 0.6, "voltage": 2e6, "phi0": -0.1, "rf_frequency": 499.98e6,
+                                             "x_offset": 1e-4, "y_pitch": 1e-4, "tilt": 0.05}, num_steps=7))
+    E.append(L.Element("marker", "MK"))
+    E.append(L.Element("quadrupole", "QOFF", {"l": 0.4, "k1": 1.0}, is_on=False))
+    E.append(L.Element("sextupole", "SOFF", {"l": 0.2, "k2": 50.0}, is_on=False))
+    if apertures:
+        E[1].aperture_type = "elliptical"
+        E[1].values.update(x1_limit=0.02, x2_limit=0.02, y1_limit=0.01, y2_limit=0.01)
+        E[5].values.update(x1_limit=0.025, x2_limit=0.02, y1_limit=0.0, y2_limit=0.012)
+        E[5].aperture_at = "both_ends"
+        E[-3].aperture_type = "elliptical"
+        E[-3].values.update(x1_limit=0.01, x2_limit=0.012, y1_limit=0.008, y2_limit=0.008)
+    lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "zoo")
+    return lat.finalize()
+
+
+def random_particles(n: int, seed: int, scale: float = 1.0) -> np.ndarray:
+    """Particles spanning a few mm / mrad / percent: (6, n)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    s = np.array([3e-3, 3e-4, 2e-3, 2e-4, 5e-3, 5e-3]) * scale
+    return rng.standard_normal((6, n)) * s[:, None]
+
+
+def rel_err(g: np.ndarray, o: np.ndarray, mask=None) -> np.ndarray:
+    """Per-coordinate max of |g - o| / (|o| + rms_c)."""
+    if mask is not None:
+        g, o = g[:, mask], o[:, mask]
+    if g.shape[1] == 0:
+        return np.zeros(6)
+    rms = np.sqrt(np.mean(o * o, axis=1))
+    return np.max(np.abs(g - o) / (np.abs(o) + rms[:, None] + 1e-300), axis=1)
+
+
+def oracle_track_elements(lat: L.Lattice, vec6: np.ndarray, start: int, stop: int, n_turns: int = 1,
+                          threads: int = 0):
+    """Oracle over elements [start, stop) (turn loop when n_turns > 1)."""
+    from oracle import oracle as O
+
+    lib = O.load()
+    sub = L.Lattice(lat.elements[start:stop], lat.species, lat.p0c, lat.e_tot)
+    eles = (O.Ele * len(sub.elements))()
+    for i, e in enumerate(sub.elements):
+        eles[i] = O.to_ele(e, lib)
+    param = O.make_param(lat.species.mass, lat.species.charge)
+    v = np.ascontiguousarray(vec6, dtype=np.float64).copy()
+    n = v.shape[1]
+    b = O.beta_of(lat.p0c, v[5], lat.species.mass)
+    st = np.ones(n, np.int32)
+    ie = np.full(n, -1, np.int32)
+    it = np.full(n, -1, np.int32)
+    O.track_turns(eles, lat.p0c, param, v, b, st, ie, it, n_turns, n_threads=threads, lib=lib)
+    return v, b, st, ie, it

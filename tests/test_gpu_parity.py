@@ -1,0 +1,181 @@
+"""GPU parity: the CUDA tracker (through the C ABI) against the CPU oracle on
+identical seeded particles.  Tolerances are stated in tests/helpers.py:
+1e-13 relative per coordinate after one element / one turn, 1e-9 after 1000
+turns; states, loss elements and loss turns exact."""
+import numpy as np
+import pytest
+
+from bgt import lattice as L
+from bgt import rings
+from bgt.track import Bunch, Tracker
+
+from helpers import (RTOL_1000_TURNS, RTOL_ONE_TURN, oracle_track_elements, random_particles, rel_err,
+                     zoo_lattice)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def zoo():
+    lat = zoo_lattice()
+    return lat, Tracker(lat)
+
+
+def test_each_element_track1(zoo):
+    lat, tr = zoo
+    v0 = random_particles(2048, seed=11)
+    for pos, ele in enumerate(lat.elements):
+        b = tr.make_bunch(v0.copy())
+        tr.track1(b, pos)
+        ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1)
+        assert np.array_equal(b.state, ost), f"{ele.name}: state mismatch"
+        alive = ost == L.ALIVE
+        err = rel_err(b.vec6, ov, alive)
+        assert np.all(err <= RTOL_ONE_TURN), f"{ele.name}: rel err {err}"
+        berr = np.max(np.abs(b.beta[alive] - ob[alive]) / ob[alive]) if alive.any() else 0
+        assert berr <= RTOL_ONE_TURN, f"{ele.name}: beta err {berr}"
+        lost = ~alive
+        assert np.array_equal(b.ix_ele_lost[lost], oie[lost]), f"{ele.name}: loss element"
+
+
+def test_zoo_pass_with_losses(zoo):
+    lat, tr = zoo
+    v0 = random_particles(4096, seed=12, scale=4.0)
+    b = tr.make_bunch(v0.copy())
+    tr.track_elements(b, 0, len(lat))
+    ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, 0, len(lat))
+    assert np.array_equal(b.state, ost)
+    assert np.array_equal(b.ix_ele_lost, oie)
+    assert (ost != L.ALIVE).sum() > 100  # the case exercises losses
+    err = rel_err(b.vec6, ov, ost == L.ALIVE)
+    assert np.all(err <= RTOL_ONE_TURN), err
+
+
+@pytest.fixture(scope="module")
+def ring():
+    lat = rings.fodo_ring()
+    return lat, Tracker(lat)
+
+
+def test_ring_one_turn(ring):
+    lat, tr = ring
+    v0 = rings.gaussian_beam(rings.CONFIG0_BEAM)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 1)
+    ov, ob, ost, _, _ = oracle_track_elements(lat, v0, 0, len(lat), 1)
+    assert np.all(b.state == L.ALIVE) and np.all(ost == L.ALIVE)
+    err = rel_err(b.vec6, ov)
+    assert np.all(err <= RTOL_ONE_TURN), err
+
+
+def test_ring_1000_turns(ring):
+    lat, tr = ring
+    v0 = rings.gaussian_beam(rings.CONFIG0_BEAM, n=1000)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 1000)
+    ov, ob, ost, _, _ = oracle_track_elements(lat, v0, 0, len(lat), 1000)
+    assert np.all(ost == L.ALIVE) and np.all(b.state == L.ALIVE)
+    err = rel_err(b.vec6, ov)
+    assert np.all(err <= RTOL_1000_TURNS), err
+
+
+def test_apertures_loss_records():
+    lat = rings.fodo_ring(apertures=True)
+    tr = Tracker(lat)
+    # a beam large enough to scrape the 20 mm x 10 mm quad apertures
+    spec = rings.BeamSpec(3000, 4e-6, 2e-6, 3e-3, 2e-3, seed=77)
+    v0 = rings.gaussian_beam(spec)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 50)
+    ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), 50)
+    n_lost = int((ost != L.ALIVE).sum())
+    assert n_lost > 50
+    assert np.array_equal(b.state, ost)
+    assert np.array_equal(b.ix_ele_lost, oie)
+    assert np.array_equal(b.ix_turn_lost, oit)
+
+
+def test_compaction_and_tiles_do_not_change_results():
+    lat = rings.fodo_ring(apertures=True)
+    spec = rings.BeamSpec(5000, 4e-6, 2e-6, 3e-3, 2e-3, seed=78)
+    v0 = rings.gaussian_beam(spec)
+    outs = []
+    for tun in (dict(threads_per_block=128, blocks_per_sm=4),
+                dict(threads_per_block=64, blocks_per_sm=8, compact_every=2, turns_per_launch=7),
+                dict(threads_per_block=256, blocks_per_sm=2, compact_every=1)):
+        tr = Tracker(lat, tuning=tun)
+        b = tr.make_bunch(v0.copy())
+        tr.track_turns(b, 30)
+        outs.append(b)
+    for o in outs[1:]:
+        assert np.array_equal(o.state, outs[0].state)
+        assert np.array_equal(o.ix_ele_lost, outs[0].ix_ele_lost)
+        assert np.array_equal(o.ix_turn_lost, outs[0].ix_turn_lost)
+        assert np.array_equal(o.vec6, outs[0].vec6)
+
+
+def test_variants_batched():
+    lats = rings.error_variants(4, seed=5)
+    tr = Tracker(lats)
+    n = 1200
+    v0 = random_particles(n, seed=13, scale=0.5)
+    var = np.arange(n, dtype=np.int32) % 4
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 3, variant=var)
+    for v in range(4):
+        m = var == v
+        ov, ob, ost, oie, oit = oracle_track_elements(lats[v], v0[:, m], 0, len(lats[v]), 3)
+        assert np.array_equal(b.state[m], ost)
+        assert np.array_equal(b.ix_ele_lost[m], oie)
+        err = rel_err(b.vec6[:, m], ov, ost == L.ALIVE)
+        assert np.all(err <= 1e-12), (v, err)
+
+
+def test_device_api_matches_host_api(ring):
+    import torch
+
+    lat, tr = ring
+    v0 = rings.gaussian_beam(rings.CONFIG0_BEAM, n=4096)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 5)
+    dv = torch.tensor(v0, dtype=torch.float64, device="cuda").contiguous()
+    db = torch.tensor(L.beta_of(lat.p0c, v0[5], lat.species.mass), device="cuda")
+    ds = torch.ones(4096, dtype=torch.int32, device="cuda")
+    de = torch.full((4096,), -1, dtype=torch.int32, device="cuda")
+    dt = torch.full((4096,), -1, dtype=torch.int32, device="cuda")
+    tr.track_turns_device(dv, db, ds, de, dt, 5)
+    torch.cuda.synchronize()
+    assert np.array_equal(dv.cpu().numpy(), b.vec6)
+    assert np.array_equal(ds.cpu().numpy(), b.state)
+
+
+def test_da_grid_matches_oracle():
+    lat = rings.fodo_ring(apertures=True)
+    tr = Tracker(lat)
+    ref = np.zeros((1, 2, 6))
+    ref[0, 1, 5] = 0.005
+    ref[0, 1, 0] = 0.005 * rings.TWISS0["eta_x"]
+    ref[0, 1, 1] = 0.005 * rings.TWISS0["etap_x"]
+    n_angle, n_radius, r_max, turns = 6, 12, 0.03, 40
+    da, surv = tr.da_scan_grid(ref, n_angle, 0.0, np.pi, n_radius, r_max, 1.0, turns, return_survival=True)
+    # oracle on the same grid
+    angs = np.linspace(0, np.pi, n_angle)
+    rads = np.arange(n_radius) * (r_max / (n_radius - 1))
+    for d in range(2):
+        pts = []
+        for a in angs:
+            for r in rads:
+                p = ref[0, d].copy()
+                p[0] += np.cos(a) * r
+                p[2] += np.sin(a) * r * 1.0
+                pts.append(p)
+        v0 = np.array(pts).T.copy()
+        ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), turns)
+        s = np.where(ost == L.ALIVE, turns, oit)
+        assert np.array_equal(surv[0, d].reshape(-1), s)
+        alive = (ost == L.ALIVE).reshape(n_angle, n_radius)
+        for ia in range(n_angle):
+            lost = np.nonzero(~alive[ia])[0]
+            first = lost[0] if lost.size else n_radius
+            expect = 0.0 if first == 0 else rads[first - 1]
+            assert abs(da[0, d, ia] - expect) < 1e-15
