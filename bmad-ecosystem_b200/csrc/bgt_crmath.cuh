@@ -1,0 +1,395 @@
+// bgt_crmath.cuh -- correctly rounded FP64 sin, cos, asin, atan2 for the
+// tracker's device code (and, compiled for the host, for testing).
+//
+// Why: the exact sector-bend map (track_a_bend.f90:163-209) cancels
+// O(L^2 g) ~ 5e-2 terms to produce O(1e-3) coordinates, so a one-ulp change
+// in sin/asin/atan2 moves the orbit by ~1e-13 relative per bend.  The
+// reference evaluates these with the platform libm (glibc), which is
+// correctly rounded in nearly every case on the arguments used here; a
+// correctly rounded device implementation therefore reproduces the
+// reference's values, where the CUDA math library (a few ulp) does not.
+//
+// Method (Ziv's strategy: fast path + rounding test + accurate path):
+//   fast path   the leading Taylor terms in double-double, the tail in
+//               double; error bound e; if both v - e and v + e round to the
+//               same double, that double is the correctly rounded result.
+//   slow path   full double-double Taylor evaluation after Cody-Waite
+//               argument reduction (sin/cos), argument halving (atan) or
+//               the half-angle identity (asin): error ~2^-100, then round.
+// Arguments beyond the documented ranges (|x| >= 2^19 for sin/cos,
+// non-finite values, extreme atan2 exponents) use the CUDA / C library
+// function.
+#pragma once
+#include <math.h>
+
+#include "bgt_crmath_tables.h"
+
+#ifdef __CUDACC__
+#define BGT_HD __host__ __device__ __forceinline__
+#else
+#define BGT_HD static inline
+#endif
+
+namespace bgt {
+namespace cr {
+
+struct dd {
+  double hi, lo;
+};
+
+BGT_HD dd two_sum(double a, double b) {
+  double s = a + b;
+  double bb = s - a;
+  return {s, (a - (s - bb)) + (b - bb)};
+}
+BGT_HD dd fast_two_sum(double a, double b) {  // |a| >= |b|
+  double s = a + b;
+  return {s, b - (s - a)};
+}
+BGT_HD dd two_prod(double a, double b) {
+  double p = a * b;
+  return {p, fma(a, b, -p)};
+}
+BGT_HD dd dd_add(dd a, dd b) {
+  dd s = two_sum(a.hi, b.hi);
+  dd t = two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = fast_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return fast_two_sum(s.hi, s.lo);
+}
+BGT_HD dd dd_add_d(dd a, double b) {
+  dd s = two_sum(a.hi, b);
+  s.lo += a.lo;
+  return fast_two_sum(s.hi, s.lo);
+}
+BGT_HD dd dd_mul(dd a, dd b) {
+  dd p = two_prod(a.hi, b.hi);
+  p.lo = fma(a.hi, b.lo, fma(a.lo, b.hi, p.lo));
+  return fast_two_sum(p.hi, p.lo);
+}
+BGT_HD dd dd_mul_d(dd a, double b) {
+  dd p = two_prod(a.hi, b);
+  p.lo = fma(a.lo, b, p.lo);
+  return fast_two_sum(p.hi, p.lo);
+}
+BGT_HD dd dd_c(const double c[2]) { return {c[0], c[1]}; }
+BGT_HD dd dd_neg(dd a) { return {-a.hi, -a.lo}; }
+BGT_HD dd dd_div(dd a, dd b) {
+  double q1 = a.hi / b.hi;
+  dd r = dd_add(a, dd_neg(dd_mul_d(b, q1)));
+  double q2 = r.hi / b.hi;
+  r = dd_add(r, dd_neg(dd_mul_d(b, q2)));
+  double q3 = r.hi / b.hi;
+  return dd_add_d(fast_two_sum(q1, q2), q3);
+}
+BGT_HD dd dd_sqrt(dd a) {
+  if (a.hi <= 0) return {sqrt(a.hi), 0.0};
+  double s = sqrt(a.hi);
+  dd sq = two_prod(s, s);
+  double r = (((a.hi - sq.hi) - sq.lo) + a.lo) / (2 * s);
+  return fast_two_sum(s, r);
+}
+
+// Round v to double if every value within +/- err of v rounds the same way.
+BGT_HD bool round_test(dd v, double err, double* out) {
+  double a = v.hi + (v.lo - err);
+  double b = v.hi + (v.lo + err);
+  if (a == b) {
+    *out = a;
+    return true;
+  }
+  return false;
+}
+
+// ---- double-double Taylor kernels on a reduced double-double argument ----
+
+// sin(r), |r| <= pi/4 + tiny
+BGT_HD dd dd_sin_kernel(dd r) {
+  dd r2 = dd_mul(r, r);
+  // Horner over k = 16 .. 1 in double-double, then * r
+  dd acc = dd_c(SIN_C[16]);
+  for (int k = 15; k >= 1; k--) acc = dd_add(dd_mul(acc, r2), dd_c(SIN_C[k]));
+  acc = dd_mul(acc, r2);  // sum_{k>=1} c_k r^(2k)
+  return dd_add(r, dd_mul(acc, r));
+}
+// cos(r), |r| <= pi/4 + tiny
+BGT_HD dd dd_cos_kernel(dd r) {
+  dd r2 = dd_mul(r, r);
+  dd acc = dd_c(COS_C[16]);
+  for (int k = 15; k >= 1; k--) acc = dd_add(dd_mul(acc, r2), dd_c(COS_C[k]));
+  acc = dd_mul(acc, r2);
+  return dd_add_d(acc, 1.0);
+}
+
+// Cody-Waite reduction x = k*pi/2 + r, |k| < 2^19; r as double-double.
+BGT_HD dd reduce_pio2(double x, int* quadrant) {
+  double k = rint(x * BGT_CR_TWO_OVER_PI);
+  // x - k*p1 is exact (k*p1 exact, Sterbenz); k*p2 exact (33-bit factors)
+  double t = x - k * BGT_CR_PIO2_CW1;
+  dd r = two_sum(t, -(k * BGT_CR_PIO2_CW2));
+  r = dd_add(r, dd_neg(two_prod(k, BGT_CR_PIO2_CW3)));
+  long long ki = (long long)k;
+  *quadrant = (int)(ki & 3);
+  return r;
+}
+
+BGT_HD void dd_sincos_any(double x, dd* s, dd* c) {
+  int q = 0;
+  dd r = (fabs(x) <= 0.78539816339744828) ? dd{x, 0.0} : reduce_pio2(x, &q);
+  dd sr = dd_sin_kernel(r), cr = dd_cos_kernel(r);
+  switch (q) {
+    case 0: *s = sr; *c = cr; break;
+    case 1: *s = cr; *c = dd_neg(sr); break;
+    case 2: *s = dd_neg(sr); *c = dd_neg(cr); break;
+    default: *s = dd_neg(cr); *c = sr; break;
+  }
+}
+
+// ---- sin / cos ----
+
+BGT_HD double sin_fast_or_nan(double x) {
+  // |x| <= pi/4: x + T3 + T5 (double-double) + x^7 P(x^2) (double)
+  dd x2 = two_prod(x, x);
+  dd x3 = dd_mul_d(x2, x);
+  dd x5 = dd_mul(x3, x2);
+  dd t3 = dd_mul(x3, dd_c(SIN_C[1]));
+  dd t5 = dd_mul(x5, dd_c(SIN_C[2]));
+  double y = x2.hi;
+  double p = SIN_C[8][0];
+  for (int k = 7; k >= 3; k--) p = p * y + SIN_C[k][0];
+  double tail = x5.hi * y * p;
+  dd acc = dd_add_d(t5, tail);
+  acc = dd_add(t3, acc);
+  acc = dd_add_d(acc, x);
+  // tail evaluation error (relative 2^-49), double-double terms (2^-96 |x|),
+  // truncation after x^17 (< x^19/19! <= 1e-17 |x| y^9)
+  double err = fabs(tail) * 0x1p-49 + fabs(x) * 0x1p-96 + fabs(x) * (y * y * y) * (y * y * y) * (y * y * y) * 1e-17;
+  double out;
+  if (round_test(acc, err, &out)) return out;
+  return NAN;
+}
+
+BGT_HD double cos_fast_or_nan(double x) {
+  dd x2 = two_prod(x, x);
+  dd x4 = dd_mul(x2, x2);
+  dd t2 = {x2.hi * COS_C[1][0], x2.lo * COS_C[1][0]};  // * (-1/2), exact
+  dd t4 = dd_mul(x4, dd_c(COS_C[2]));
+  double y = x2.hi;
+  double p = COS_C[9][0];
+  for (int k = 8; k >= 3; k--) p = p * y + COS_C[k][0];
+  double tail = x4.hi * y * p;
+  dd acc = dd_add_d(t4, tail);
+  acc = dd_add(t2, acc);
+  acc = dd_add_d(acc, 1.0);
+  double err = fabs(tail) * 0x1p-49 + 0x1p-100 + (y * y * y) * (y * y * y) * (y * y * y) * y * 1e-18;
+  double out;
+  if (round_test(acc, err, &out)) return out;
+  return NAN;
+}
+
+BGT_HD double sin(double x) {
+  if (!(fabs(x) < 524288.0)) return ::sin(x);  // non-finite or huge: library value
+  if (x == 0) return x;
+  if (fabs(x) <= 0.78539816339744828) {
+    double f = sin_fast_or_nan(x);
+    if (f == f) return f;
+  }
+  dd s, c;
+  dd_sincos_any(x, &s, &c);
+  return s.hi + s.lo;
+}
+
+BGT_HD double cos(double x) {
+  if (!(fabs(x) < 524288.0)) return ::cos(x);
+  if (fabs(x) <= 0.78539816339744828) {
+    double f = cos_fast_or_nan(x);
+    if (f == f) return f;
+  }
+  dd s, c;
+  dd_sincos_any(x, &s, &c);
+  return c.hi + c.lo;
+}
+
+BGT_HD void sincos(double x, double* s, double* c) {
+  *s = cr::sin(x);
+  *c = cr::cos(x);
+}
+
+// ---- sinh / cosh (|x| <= 2; larger arguments use the library) ----
+
+BGT_HD dd dd_sinh_kernel(double x) {
+  dd x2 = two_prod(x, x);
+  dd acc = dd_c(SINH_C[16]);
+  for (int k = 15; k >= 1; k--) acc = dd_add(dd_mul(acc, x2), dd_c(SINH_C[k]));
+  acc = dd_mul(acc, x2);
+  return dd_add_d(dd_mul_d(acc, x), x);
+}
+BGT_HD dd dd_cosh_kernel(double x) {
+  dd x2 = two_prod(x, x);
+  dd acc = dd_c(COSH_C[16]);
+  for (int k = 15; k >= 1; k--) acc = dd_add(dd_mul(acc, x2), dd_c(COSH_C[k]));
+  acc = dd_mul(acc, x2);
+  return dd_add_d(acc, 1.0);
+}
+
+BGT_HD double sinh(double x) {
+  double a = fabs(x);
+  if (!(a <= 2.0)) return ::sinh(x);
+  if (x == 0) return x;
+  if (a <= 0.78539816339744828) {
+    dd x2 = two_prod(x, x);
+    dd x3 = dd_mul_d(x2, x);
+    dd x5 = dd_mul(x3, x2);
+    dd t3 = dd_mul(x3, dd_c(SINH_C[1]));
+    dd t5 = dd_mul(x5, dd_c(SINH_C[2]));
+    double y = x2.hi;
+    double p = SINH_C[8][0];
+    for (int k = 7; k >= 3; k--) p = p * y + SINH_C[k][0];
+    double tail = x5.hi * y * p;
+    dd acc = dd_add_d(t5, tail);
+    acc = dd_add(t3, acc);
+    acc = dd_add_d(acc, x);
+    double err = fabs(tail) * 0x1p-49 + a * 0x1p-96 + a * (y * y * y) * (y * y * y) * (y * y * y) * 1e-17;
+    double out;
+    if (round_test(acc, err, &out)) return out;
+  }
+  dd r = dd_sinh_kernel(x);
+  return r.hi + r.lo;
+}
+
+BGT_HD double cosh(double x) {
+  double a = fabs(x);
+  if (!(a <= 2.0)) return ::cosh(x);
+  if (a <= 0.78539816339744828) {
+    dd x2 = two_prod(x, x);
+    dd x4 = dd_mul(x2, x2);
+    dd t2 = {x2.hi * COSH_C[1][0], x2.lo * COSH_C[1][0]};  // * (1/2), exact
+    dd t4 = dd_mul(x4, dd_c(COSH_C[2]));
+    double y = x2.hi;
+    double p = COSH_C[9][0];
+    for (int k = 8; k >= 3; k--) p = p * y + COSH_C[k][0];
+    double tail = x4.hi * y * p;
+    dd acc = dd_add_d(t4, tail);
+    acc = dd_add(t2, acc);
+    acc = dd_add_d(acc, 1.0);
+    double err = fabs(tail) * 0x1p-49 + 0x1p-100 + (y * y * y) * (y * y * y) * (y * y * y) * y * 1e-18;
+    double out;
+    if (round_test(acc, err, &out)) return out;
+  }
+  dd r = dd_cosh_kernel(x);
+  return r.hi + r.lo;
+}
+
+// ---- asin ----
+
+// asin(r) for a double-double r with |r| <= 1/2, full double-double series.
+BGT_HD dd dd_asin_kernel(dd r) {
+  dd r2 = dd_mul(r, r);
+  dd acc = dd_c(ASIN_C[39]);
+  for (int k = 38; k >= 1; k--) acc = dd_add(dd_mul(acc, r2), dd_c(ASIN_C[k]));
+  acc = dd_mul(acc, r2);
+  return dd_add(r, dd_mul(acc, r));
+}
+
+BGT_HD double asin(double u) {
+  double a = fabs(u);
+  if (!(a <= 1.0)) return ::asin(u);  // |u| > 1 or NaN
+  if (u == 0) return u;
+  if (a <= 0.125) {
+    dd u2 = two_prod(u, u);
+    dd u3 = dd_mul_d(u2, u);
+    dd u5 = dd_mul(u3, u2);
+    dd t3 = dd_mul(u3, dd_c(ASIN_C[1]));
+    dd t5 = dd_mul(u5, dd_c(ASIN_C[2]));
+    double y = u2.hi;
+    double p = ASIN_C[12][0];
+    for (int k = 11; k >= 3; k--) p = p * y + ASIN_C[k][0];
+    double tail = u5.hi * y * p;
+    dd acc = dd_add_d(t5, tail);
+    acc = dd_add(t3, acc);
+    acc = dd_add_d(acc, u);
+    // truncation after u^25: < 0.02 u y^12 / (1 - y)
+    double y4 = y * y * y * y;
+    double err = fabs(tail) * 0x1p-49 + a * 0x1p-96 + a * y4 * y4 * y4 * 0.03;
+    double out;
+    if (round_test(acc, err, &out)) return out;
+  }
+  dd r;
+  if (a <= 0.5) {
+    r = dd_asin_kernel({a, 0.0});
+  } else {
+    // asin(a) = pi/2 - 2 asin(sqrt((1 - a) / 2)), (1 - a)/2 exact for a >= 1/2
+    double z = (1.0 - a) * 0.5;
+    dd s = dd_sqrt({z, 0.0});
+    dd as = dd_asin_kernel(s);
+    r = dd_add(dd{BGT_CR_PIO2_HI, BGT_CR_PIO2_LO}, dd_neg(dd_mul_d(as, 2.0)));
+  }
+  double v = r.hi + r.lo;
+  return u < 0 ? -v : v;
+}
+
+// ---- atan2 ----
+
+// atan(q) for a double-double q with |q| <= 1, via two argument halvings
+// atan(q) = 2 atan(q / (1 + sqrt(1 + q^2))) and the series.
+BGT_HD dd dd_atan_kernel(dd q) {
+  int halvings = 0;
+  while (fabs(q.hi) > 0.1 && halvings < 4) {
+    dd den = dd_add_d(dd_sqrt(dd_add_d(dd_mul(q, q), 1.0)), 1.0);
+    q = dd_div(q, den);
+    halvings++;
+  }
+  dd q2 = dd_mul(q, q);
+  dd acc = dd_c(ATAN_C[39]);
+  for (int k = 38; k >= 1; k--) acc = dd_add(dd_mul(acc, q2), dd_c(ATAN_C[k]));
+  acc = dd_mul(acc, q2);
+  dd r = dd_add(q, dd_mul(acc, q));
+  for (int h = 0; h < halvings; h++) r = dd_mul_d(r, 2.0);
+  return r;
+}
+
+BGT_HD double atan2(double y, double x) {
+  if (!(fabs(x) < 1e300 && fabs(y) < 1e300) || x == 0 || y == 0) return ::atan2(y, x);
+  double ax = fabs(x), ay = fabs(y);
+  if (ay > ax * 0x1p60 || ay < ax * 0x1p-60) return ::atan2(y, x);
+  // q = y / x as double-double (exact remainder by fma)
+  double qh = y / x;
+  double ql = fma(-qh, x, y) / x;
+  if (x > 0 && fabs(qh) <= 0.125) {
+    dd q2 = two_prod(qh, qh);
+    dd q3 = dd_mul_d(q2, qh);
+    dd q5 = dd_mul(q3, q2);
+    dd t3 = dd_mul(q3, dd_c(ATAN_C[1]));
+    dd t5 = dd_mul(q5, dd_c(ATAN_C[2]));
+    double yy = q2.hi;
+    double p = ATAN_C[11][0];
+    for (int k = 10; k >= 3; k--) p = p * yy + ATAN_C[k][0];
+    double tail = q5.hi * yy * p;
+    double corr = ql / (1.0 + yy);  // d atan = dq / (1 + q^2)
+    dd acc = dd_add_d(t5, tail);
+    acc = dd_add(t3, acc);
+    acc = dd_add_d(acc, corr);
+    acc = dd_add_d(acc, qh);
+    double y4 = yy * yy * yy * yy;
+    double err = fabs(tail) * 0x1p-49 + fabs(corr) * 0x1p-50 + fabs(qh) * 0x1p-96 +
+                 fabs(qh) * y4 * y4 * y4 * 0.05;
+    double out;
+    if (round_test(acc, err, &out)) return out;
+  }
+  dd q = {qh, ql};
+  dd a;
+  if (fabs(qh) <= 1.0) {
+    a = dd_atan_kernel(q);
+  } else {
+    dd inv = dd_div({1.0, 0.0}, q);
+    dd b = dd_atan_kernel(inv);
+    dd hp = dd{BGT_CR_PIO2_HI, BGT_CR_PIO2_LO};
+    a = qh > 0 ? dd_add(hp, dd_neg(b)) : dd_add(dd_neg(hp), dd_neg(b));
+  }
+  if (x < 0) a = (y >= 0) ? dd_add(a, dd{BGT_CR_PI_HI, BGT_CR_PI_LO}) : dd_add(a, dd_neg(dd{BGT_CR_PI_HI, BGT_CR_PI_LO}));
+  return a.hi + a.lo;
+}
+
+}  // namespace cr
+}  // namespace bgt

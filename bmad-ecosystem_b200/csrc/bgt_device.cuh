@@ -8,7 +8,12 @@
 #pragma once
 #include <stdint.h>
 
+#include "bgt_crmath.cuh"
 #include "bgt_table.h"
+
+// Every transcendental of a particle coordinate goes through bgt::cr
+// (correctly rounded, see bgt_crmath.cuh); element constants arrive from the
+// host table, evaluated there with the host C library.
 
 namespace bgt {
 
@@ -53,7 +58,7 @@ __device__ __forceinline__ double sqrt_one(double x) {
 // sim_utils/special_functions/sinc.f90:15-45
 __device__ __forceinline__ double sinc_d(double x) {
   if (fabs(x) < 1e-8) return 1.0;
-  return sin(x) / x;
+  return cr::sin(x) / x;
 }
 
 // x**m as gfortran evaluates it (libgcc __powidf2 order of multiplies).
@@ -358,13 +363,11 @@ __device__ __forceinline__ QMat quad_mat2_calc(double k1, double length, double 
     cx = 1 + k_l2 / 2;
     sx = (1 + k_l2 / 6) * length;
   } else if (k1 < 0) {
-    double s, c;
-    sincos(sk_l, &s, &c);
-    cx = c;
-    sx = s / sqrt_k;
+    cx = cr::cos(sk_l);
+    sx = cr::sin(sk_l) / sqrt_k;
   } else {
-    cx = cosh(sk_l);
-    sx = sinh(sk_l) / sqrt_k;
+    cx = cr::cosh(sk_l);
+    sx = cr::sinh(sk_l) / sqrt_k;
   }
   q.cx = cx;
   q.m01 = sx / rel_p;

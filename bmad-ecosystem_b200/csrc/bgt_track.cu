@@ -237,7 +237,7 @@ __device__ __forceinline__ void body_rf(Part& p, const Rec& R, const Glob& G, Dr
   const int n_slice = R.h->n_step;
   const double slice_l = q[RF_SLICE_L];
   for (int i = 0; i <= n_slice; i++) {
-    double dE = 1 * voltage * sin(phase) / n_slice;
+    double dE = 1 * voltage * cr::sin(phase) / n_slice;
     if (i == 0 || i == n_slice) dE = dE / 2;
     apply_energy_kick(p, dE, G);
     if (p.pz == -1) {
@@ -305,12 +305,12 @@ __device__ __forceinline__ void sbend_k1_body(Part& p, const double* q) {
     c_x = 1 + tau_x * (arg * arg) / 2;
     z2 = g * (length * length) / (2 * rel_p);
   } else if (k_x > 0) {
-    s_x = sin(arg) / om_x;
-    c_x = cos(arg);
+    s_x = cr::sin(arg) / om_x;
+    c_x = cr::cos(arg);
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   } else {
-    s_x = sinh(arg) / om_x;
-    c_x = cosh(arg);
+    s_x = cr::sinh(arg) / om_x;
+    c_x = cr::cosh(arg);
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   }
   arg = om_y * length;
@@ -318,11 +318,11 @@ __device__ __forceinline__ void sbend_k1_body(Part& p, const double* q) {
     s_y = (1 + tau_y * (arg * arg) / 6) * length;
     c_y = 1 + tau_y * (arg * arg) / 2;
   } else if (k1 < 0) {
-    s_y = sin(om_y * length) / om_y;
-    c_y = cos(om_y * length);
+    s_y = cr::sin(om_y * length) / om_y;
+    c_y = cr::cos(om_y * length);
   } else {
-    s_y = sinh(om_y * length) / om_y;
-    c_y = cosh(om_y * length);
+    s_y = cr::sinh(om_y * length) / om_y;
+    c_y = cr::cosh(om_y * length);
   }
   double r0 = p.x - x_c, r1 = p.px, r2 = p.y, r3 = p.py, r4 = p.z;
   double z0 = -g * x_c * length;
@@ -385,9 +385,8 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
           return;
         }
         double g_p = g_tot / pt;
-        double phi_1 = asin(px / pt);
-        double sin_plus, cos_plus;
-        sincos(angle + phi_1, &sin_plus, &cos_plus);
+        double phi_1 = cr::asin(px / pt);
+        double sin_plus = cr::sin(angle + phi_1), cos_plus = cr::cos(angle + phi_1);
         double gx1 = 1 + g * x;
         double t1 = gx1 * step_len * sinc_a;
         double alpha = 2 * gx1 * sin_plus * step_len * sinc_a - g_p * (t1 * t1);
@@ -412,9 +411,9 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
         double L_u = xi;
         double L_v = -(q[B_LLSINC] + x * q[B_SINA]);
         double L_c = sqrt(L_v * L_v + L_u * L_u);
-        double angle_p = 2 * (angle + phi_1 - 1 * atan2(L_u, -L_v));
+        double angle_p = 2 * (angle + phi_1 - 1 * cr::atan2(L_u, -L_v));
         double L_p = 1 * L_c / sinc_d(angle_p / 2);
-        p.px = pt * sin(phi_1 + angle - angle_p);
+        p.px = pt * cr::sin(phi_1 + angle - angle_p);
         p.y = y + py * L_p / pt;
         p.z = z + p.beta * step_len / q[B_BETAREF] - rel_p * L_p / pt;
       }
@@ -1561,6 +1560,7 @@ namespace bgt {
 
 struct DAArgs {
   const double* ref;  // [(v*n_delta + d)*6 + c]
+  const double* cs;   // [a] = (cos(angle_a), sin(angle_a)), host-evaluated
   int32_t n_var, n_delta, n_angle, n_radius;
   double a0, da, dr, y_scale;
   int32_t block;
@@ -1586,10 +1586,9 @@ __global__ void da_init_kernel(DAArgs A, int64_t n) {
   int32_t d = (int32_t)(q % A.n_delta);
   int32_t v = (int32_t)(q / A.n_delta);
   const double* ref = A.ref + ((int64_t)v * A.n_delta + d) * 6;
-  double ang = A.a0 + A.da * a;
   double rad = A.dr * r;
-  double x1 = cos(ang) * rad;
-  double y1 = sin(ang) * rad * A.y_scale;
+  double x1 = A.cs[2 * a] * rad;
+  double y1 = A.cs[2 * a + 1] * rad * A.y_scale;
   A.vec6[0 * A.stride + i] = ref[0] + x1;
   A.vec6[1 * A.stride + i] = ref[1];
   A.vec6[2 * A.stride + i] = ref[2] + y1;
@@ -1686,6 +1685,18 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
   double* d_da = nullptr;
   int32_t* d_surv = nullptr;
   int64_t n_rays = (int64_t)n_variants_used * n_delta * n_angle;
+  // ray directions: angle_j = j * delta_angle + min_angle
+  // (dynamic_aperture_mod.f90:88-95), cos/sin by the host C library
+  std::vector<double> cs(2 * (size_t)n_angle);
+  for (int j = 0; j < n_angle; j++) {
+    double ang = (n_angle == 1) ? (angle_min + angle_max) / 2 : j * A.da + angle_min;
+    cs[2 * j] = cos(ang);
+    cs[2 * j + 1] = sin(ang);
+  }
+  double* d_cs = nullptr;
+  CU(h, cudaMalloc(&d_cs, cs.size() * 8));
+  CU(h, cudaMemcpy(d_cs, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice));
+  A.cs = d_cs;
   CU(h, cudaMalloc(&d_ref, (size_t)n_variants_used * n_delta * 6 * 8));
   CU(h, cudaMalloc(&d_da, (size_t)n_rays * 8));
   if (survive_turns) CU(h, cudaMalloc(&d_surv, (size_t)n * 4));
@@ -1709,6 +1720,7 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
     cudaFree(d_ref);
     cudaFree(d_da);
     cudaFree(d_surv);
+    cudaFree(d_cs);
     return rc;
   }
   da_reduce_kernel<<<(unsigned)((n_rays + 127) / 128), 128>>>(d_state, d_ixt, n_rays, n_radius, A.dr, 0, n_turns,
@@ -1722,6 +1734,7 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
   cudaFree(d_ref);
   cudaFree(d_da);
   cudaFree(d_surv);
+  cudaFree(d_cs);
   if (flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete");
   return 0;
 }

@@ -54,6 +54,26 @@ void bgo_flop_counter_read(double* flops, double* libm_calls) {
 
 static double sq(double x) { return x * x; }
 
+/* Transcendentals of particle coordinates.  The default build calls the C
+ * library (as the reference does); the BGO_CR_LIBM build rounds libquadmath's
+ * quad-precision values to double, i.e. correctly rounded results.  Element
+ * constants (tilts, bend angles, edge angles) always use the C library. */
+#ifdef BGO_CR_LIBM
+static double P_SIN(double x) { return (double)sinq((__float128)x); }
+static double P_COS(double x) { return (double)cosq((__float128)x); }
+static double P_ASIN(double x) { return (double)asinq((__float128)x); }
+static double P_ATAN2(double y, double x) { return (double)atan2q((__float128)y, (__float128)x); }
+static double P_SINH(double x) { return (double)sinhq((__float128)x); }
+static double P_COSH(double x) { return (double)coshq((__float128)x); }
+#else
+#define P_SIN sin
+#define P_COS cos
+#define P_ASIN asin
+#define P_ATAN2 atan2
+#define P_SINH sinh
+#define P_COSH cosh
+#endif
+
 /* x**m for integer m, as gfortran evaluates it (repeated squaring,
  * libgcc __powidf2 / libgfortran pow_r8_i4 order of multiplies). */
 static double powi_f(double x, int m) {
@@ -84,6 +104,14 @@ static double sinc_f(double x) {
   LM(1);
   FL(1);
   return sin(x) / x;
+}
+
+/* sinc of a particle-dependent argument */
+static double sinc_p(double x) {
+  if (fabs(x) < 1e-8) return 1.0;
+  LM(1);
+  FL(1);
+  return P_SIN(x) / x;
 }
 
 /* sim_utils/special_functions/cosc.f90:15-35 (nd = 0) */
@@ -1306,13 +1334,13 @@ static void quad_mat2_calc(double k1, double length, double rel_p, double m[2][2
     sx = (1 + k_l2 / 6) * length;
     FL(8);
   } else if (k1 < 0) {
-    cx = cos(sk_l);
-    sx = sin(sk_l) / sqrt_k;
+    cx = P_COS(sk_l);
+    sx = P_SIN(sk_l) / sqrt_k;
     LM(2);
     FL(1);
   } else {
-    cx = cosh(sk_l);
-    sx = sinh(sk_l) / sqrt_k;
+    cx = P_COSH(sk_l);
+    sx = P_SINH(sk_l) / sqrt_k;
     LM(2);
     FL(1);
   }
@@ -1473,12 +1501,12 @@ static void sbend_body_with_k1_map(const bgo_ele* ele, double dg, double b1, int
     c_x = 1 + tau_x * (arg * arg) / 2;
     z2 = g * (length * length) / (2 * rel_p);
   } else if (k_x > 0) {
-    s_x = sin(arg) / om_x;
-    c_x = cos(arg);
+    s_x = P_SIN(arg) / om_x;
+    c_x = P_COS(arg);
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   } else {
-    s_x = sinh(arg) / om_x;
-    c_x = cosh(arg);
+    s_x = P_SINH(arg) / om_x;
+    c_x = P_COSH(arg);
     z2 = tau_x * g * (1 - c_x) / (rel_p * (om_x * om_x));
   }
   arg = om_y * length;
@@ -1486,11 +1514,11 @@ static void sbend_body_with_k1_map(const bgo_ele* ele, double dg, double b1, int
     s_y = (1 + tau_y * (arg * arg) / 6) * length;
     c_y = 1 + tau_y * (arg * arg) / 2;
   } else if (k1 < 0) {
-    s_y = sin(om_y * length) / om_y;
-    c_y = cos(om_y * length);
+    s_y = P_SIN(om_y * length) / om_y;
+    c_y = P_COS(om_y * length);
   } else {
-    s_y = sinh(om_y * length) / om_y;
-    c_y = cosh(om_y * length);
+    s_y = P_SINH(om_y * length) / om_y;
+    c_y = P_COSH(om_y * length);
   }
   double r[6];
   for (int i = 0; i < 6; i++) r[i] = orbit->vec[i];
@@ -1615,9 +1643,9 @@ static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) 
           return 0;
         }
         double g_p = g_tot / pt;
-        double phi_1 = asin(px / pt);
+        double phi_1 = P_ASIN(px / pt);
         double cos_a = cos(angle), sin_a = sin(angle), cosc_a = cosc_f(angle);
-        double cos_plus = cos(angle + phi_1), sin_plus = sin(angle + phi_1);
+        double cos_plus = P_COS(angle + phi_1), sin_plus = P_SIN(angle + phi_1);
         double gx1 = 1 + g * x;
         double alpha = 2 * gx1 * sin_plus * step_len * sinc_a - g_p * sq(gx1 * step_len * sinc_a);
         double r = cos_plus * cos_plus + g_p * alpha;
@@ -1645,9 +1673,9 @@ static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) 
         double L_u = xi;
         double L_v = -(step_len * sinc_a + x * sin_a);
         double L_c = sqrt(L_v * L_v + L_u * L_u);
-        double angle_p = 2 * (angle + phi_1 - 1 * atan2(L_u, -L_v));
-        double L_p = 1 * L_c / sinc_f(angle_p / 2);
-        orbit->vec[1] = pt * sin(phi_1 + angle - angle_p);
+        double angle_p = 2 * (angle + phi_1 - 1 * P_ATAN2(L_u, -L_v));
+        double L_p = 1 * L_c / sinc_p(angle_p / 2);
+        orbit->vec[1] = pt * P_SIN(phi_1 + angle - angle_p);
         orbit->vec[2] = y + py * L_p / pt;
         orbit->vec[4] = z + orbit->beta * step_len / beta_ref - rel_p * L_p / pt;
         LM(2);
@@ -1703,7 +1731,7 @@ static int track_a_rfcavity(bgo_coord* orbit, const bgo_ele* ele, const bgo_para
   FL(8);
 
   for (int i = 0; i <= n_slice; i++) {
-    double dE = 1 * voltage * sin(phase) / n_slice;
+    double dE = 1 * voltage * P_SIN(phase) / n_slice;
     if (i == 0 || i == n_slice) dE = dE / 2;
     LM(1);
     FL(3);

@@ -54,8 +54,8 @@ class Ele(C.Structure):
         (n, C.c_double * N_POLE) for n in ("a_pole", "b_pole", "ksl_pole", "a_pole_elec", "b_pole_elec")]
 
 
-_lib = None
-_lib_count = None
+_libs = {}
+VARIANTS = {"glibc": "liboracle.so", "count": "liboracle_count.so", "cr": "liboracle_cr.so"}
 
 
 def build():
@@ -83,19 +83,19 @@ def _bind(lib):
     return lib
 
 
-def load(count_flops: bool = False):
-    global _lib, _lib_count
-    name = "liboracle_count.so" if count_flops else "liboracle.so"
-    if (count_flops and _lib_count is None) or (not count_flops and _lib is None):
-        path = BUILD / name
+def load(count_flops: bool = False, variant: str = "glibc"):
+    """The oracle library.  variant "glibc": transcendentals from the C library,
+    as the reference evaluates them; "cr": transcendentals of particle
+    coordinates correctly rounded; "count": glibc build with FP64 operation
+    counters (single thread)."""
+    if count_flops:
+        variant = "count"
+    if variant not in _libs:
+        path = BUILD / VARIANTS[variant]
         if not path.exists():
             build()
-        lib = _bind(C.CDLL(str(path)))
-        if count_flops:
-            _lib_count = lib
-        else:
-            _lib = lib
-    return _lib_count if count_flops else _lib
+        _libs[variant] = _bind(C.CDLL(str(path)))
+    return _libs[variant]
 
 
 def make_param(mass: float, charge: int = -1, aperture_limit_on: bool = True) -> Param:

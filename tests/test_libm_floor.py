@@ -1,0 +1,34 @@
+"""The reference's libm sensitivity, measured on the CPU alone: the oracle
+built with the C library (as the reference runs) against the same oracle
+with correctly rounded transcendentals.  Their difference is the floor any
+implementation that does not reproduce glibc's exact rounding sees; the GPU
+tracker is bit-identical to the correctly rounded build (test_gpu_parity)."""
+import numpy as np
+
+from bgt import rings
+from helpers import RTOL_LIBM_ONE_TURN, oracle_track_elements, rel_err
+
+
+def test_cr_oracle_vs_glibc_oracle_one_turn():
+    lat = rings.fodo_ring()
+    v0 = rings.gaussian_beam(rings.CONFIG0_BEAM, n=2000)
+    cv, *_ = oracle_track_elements(lat, v0, 0, len(lat), 1, variant="cr")
+    gv, *_ = oracle_track_elements(lat, v0, 0, len(lat), 1, variant="glibc")
+    err = rel_err(cv, gv)
+    # the two CPU builds differ (glibc is not always correctly rounded) ...
+    assert np.max(err) > 1e-14
+    # ... by no more than the stated floor
+    assert np.all(err <= RTOL_LIBM_ONE_TURN), err
+
+
+def test_cr_oracle_passes_the_golden_vectors():
+    import test_oracle_golden as G
+    from oracle import oracle as O
+
+    lib = O.load(variant="cr")
+    for name in sorted(G.ELEMENTS):
+        lat = G.make_element(name)
+        ele = O.to_ele(lat.elements[0], lib)
+        param = O.make_param(G.L.M_ELECTRON, +1)
+        vec, beta, state = O.track1(ele, G.START, lat.p0c, param, lib=lib)
+        G.check_row(name, vec, G.GOLD["tracking_method"][name])
