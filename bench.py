@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
+    ap.add_argument("--tuning", default="", help="threads_per_block,blocks_per_sm (skips the autotuner)")
     return ap.parse_args()
 
 
@@ -214,6 +216,18 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     T = args.turns_per_step
+    tune_info = None
+    if args.tuning:
+        tpb, bps = (int(x) for x in args.tuning.split(","))
+        tr.set_tuning(threads_per_block=tpb, blocks_per_sm=bps)
+    elif not args.no_autotune:
+        from bgt import autotune
+
+        autotune.tune(tr, v0, turns=2, sample=min(n, 300_000))
+        res = autotune.last_results(tr, n)
+        tune_info = {"sample": res["sample"], "turns": res["turns"],
+                     "candidates_ms": [[round(ms, 3), t["threads_per_block"], t["blocks_per_sm"]]
+                                       for ms, t in res["all"]]}
 
     def barrier():
         if dist:
@@ -301,7 +315,7 @@ def main():
                            "particles_per_gpu": n, "turns_per_step": T, "parallelism": f"particles x{world} GPUs",
                            "l2": "flushed between timed steps (256 MB write)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary(), "tuning": tr.get_tuning()}
+                "clocks": clk.summary(), "tuning": tr.get_tuning(), "autotune": tune_info}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -1,0 +1,92 @@
+"""Launch-shape autotuner for the tracking kernel.
+
+Candidates are the (particles per CTA, resident CTAs per SM) pairs the library
+is compiled for -- i.e. register caps of 128/96/80/64 per thread traded
+against occupancy -- and, for lossy workloads, the compaction interval.  Each
+candidate tracks a sample of the real bunch for a few turns on the device
+(CUDA events on the launching stream); the fastest per particle.turn wins.
+Results are cached per (table bytes, lattice name, particle count) in memory
+and, when a path is given, in a JSON file.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+from typing import Dict, Iterable, Optional, Tuple
+
+import numpy as np
+
+SHAPES: Tuple[Tuple[int, int], ...] = ((64, 8), (64, 10), (64, 12), (64, 16), (128, 4), (128, 5), (128, 6),
+                                       (128, 8), (256, 2), (256, 3), (256, 4))
+
+_cache: Dict[str, dict] = {}
+
+
+def _key(tracker, n: int, lossy: bool) -> str:
+    return f"{tracker.lattice.name}:{tracker.table_bytes()}:{tracker.n_variants}:{n}:{int(lossy)}"
+
+
+def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, int]] = SHAPES,
+         compact_options: Iterable[int] = (0,), sample: int = 200_000, cache_file: Optional[str] = None,
+         verbose: bool = False) -> dict:
+    """Pick the fastest tuning for tracking `vec6` (6, n) with `tracker`;
+    sets it on the tracker and returns it."""
+    import torch
+
+    n = vec6.shape[1]
+    lossy = any(c > 0 for c in compact_options)
+    key = _key(tracker, n, lossy)
+    if cache_file and not _cache and os.path.exists(cache_file):
+        try:
+            _cache.update(json.loads(Path(cache_file).read_text()))
+        except (OSError, ValueError):
+            pass
+    if key in _cache:
+        tracker.set_tuning(**_cache[key]["tuning"])
+        return _cache[key]["tuning"]
+
+    m = min(n, sample)
+    dev = torch.device("cuda", tracker.device)
+    base = torch.tensor(np.ascontiguousarray(vec6[:, :m]), dtype=torch.float64, device=dev)
+    pz = base[5]
+    pc = (1 + pz) * tracker.p0c
+    beta0 = pc / torch.sqrt(pc * pc + tracker.species.mass ** 2)
+    stream = torch.cuda.current_stream(dev)
+    results = []
+    for (tpb, bps) in shapes:
+        for ce in compact_options:
+            tun = dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0)
+            tracker.set_tuning(**tun)
+            best = None
+            for rep in range(2):  # first repetition warms up
+                v = base.clone()
+                b = beta0.clone()
+                st = torch.ones(m, dtype=torch.int32, device=dev)
+                ie = torch.full((m,), -1, dtype=torch.int32, device=dev)
+                it = torch.full((m,), -1, dtype=torch.int32, device=dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                tracker.track_turns_device(v, b, st, ie, it, turns, stream=stream)
+                e1.record(stream)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            results.append((best, tun))
+            if verbose:
+                print(f"  tune {tun}: {best:.3f} ms")
+    results.sort(key=lambda r: r[0])
+    choice = results[0][1]
+    tracker.set_tuning(**choice)
+    _cache[key] = {"tuning": choice, "ms": results[0][0], "turns": turns, "sample": m,
+                   "all": [(ms, t) for ms, t in results]}
+    if cache_file:
+        try:
+            Path(cache_file).write_text(json.dumps(_cache, indent=1))
+        except OSError:
+            pass
+    return choice
+
+
+def last_results(tracker, n: int, lossy: bool = False) -> Optional[dict]:
+    return _cache.get(_key(tracker, n, lossy))

@@ -26,8 +26,11 @@
 
 #ifdef __CUDACC__
 #define BGT_HD __host__ __device__ __forceinline__
+// accurate paths run rarely: kept out of line so the hot loop stays small
+#define BGT_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define BGT_HD static inline
+#define BGT_HD_NOINLINE static __attribute__((noinline))
 #endif
 
 namespace bgt {
@@ -134,7 +137,7 @@ BGT_HD dd reduce_pio2(double x, int* quadrant) {
   return r;
 }
 
-BGT_HD void dd_sincos_any(double x, dd* s, dd* c) {
+BGT_HD_NOINLINE void dd_sincos_any(double x, dd* s, dd* c) {
   int q = 0;
   dd r = (fabs(x) <= 0.78539816339744828) ? dd{x, 0.0} : reduce_pio2(x, &q);
   dd sr = dd_sin_kernel(r), cr = dd_cos_kernel(r);
@@ -218,14 +221,14 @@ BGT_HD void sincos(double x, double* s, double* c) {
 
 // ---- sinh / cosh (|x| <= 2; larger arguments use the library) ----
 
-BGT_HD dd dd_sinh_kernel(double x) {
+BGT_HD_NOINLINE dd dd_sinh_kernel(double x) {
   dd x2 = two_prod(x, x);
   dd acc = dd_c(SINH_C[16]);
   for (int k = 15; k >= 1; k--) acc = dd_add(dd_mul(acc, x2), dd_c(SINH_C[k]));
   acc = dd_mul(acc, x2);
   return dd_add_d(dd_mul_d(acc, x), x);
 }
-BGT_HD dd dd_cosh_kernel(double x) {
+BGT_HD_NOINLINE dd dd_cosh_kernel(double x) {
   dd x2 = two_prod(x, x);
   dd acc = dd_c(COSH_C[16]);
   for (int k = 15; k >= 1; k--) acc = dd_add(dd_mul(acc, x2), dd_c(COSH_C[k]));
@@ -284,7 +287,7 @@ BGT_HD double cosh(double x) {
 // ---- asin ----
 
 // asin(r) for a double-double r with |r| <= 1/2, full double-double series.
-BGT_HD dd dd_asin_kernel(dd r) {
+BGT_HD_NOINLINE dd dd_asin_kernel(dd r) {
   dd r2 = dd_mul(r, r);
   dd acc = dd_c(ASIN_C[39]);
   for (int k = 38; k >= 1; k--) acc = dd_add(dd_mul(acc, r2), dd_c(ASIN_C[k]));
@@ -333,7 +336,7 @@ BGT_HD double asin(double u) {
 
 // atan(q) for a double-double q with |q| <= 1, via two argument halvings
 // atan(q) = 2 atan(q / (1 + sqrt(1 + q^2))) and the series.
-BGT_HD dd dd_atan_kernel(dd q) {
+BGT_HD_NOINLINE dd dd_atan_kernel(dd q) {
   int halvings = 0;
   while (fabs(q.hi) > 0.1 && halvings < 4) {
     dd den = dd_add_d(dd_sqrt(dd_add_d(dd_mul(q, q), 1.0)), 1.0);

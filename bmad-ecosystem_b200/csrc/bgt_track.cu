@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/bgt.h"
@@ -56,8 +57,20 @@ __device__ __forceinline__ Rec decode(const double* r) {
   return R;
 }
 
+// Per-thread memo of quad_mat2_calc results for up to QMEMO_CLASSES quad
+// strength classes (same b1, length and step), in shared memory:
+// qm[(cls * 13 + j) * stride], j = 0..11 the two QMat, j = 12 the rel_p key.
+// quad_mat2_calc is a pure function of (b1, length, step, rel_p) and rel_p
+// changes only at energy kicks, so ring quads of one class reuse it until the
+// next RF pass: value-identical, ~2 evaluations per turn instead of 128.
+constexpr int QMEMO_CLASSES = 2;
+struct QMemo {
+  double* q;  // this thread's column
+  int stride;
+};
+
 // bmad/low_level/track_a_quadrupole.f90:134-265 (magnetic, no fringe)
-__device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, DriftMemo& m) {
+__device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, DriftMemo& m, QMemo qm) {
   const double* q = R.kb;
   const int32_t fl = R.h->flags;
   const int ix = R.h->ix_mag_max;
@@ -74,9 +87,24 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
   for (int i = 1; i <= n_step; i++) {
     double rel_p = 1 + p.pz;
     if (!(rel_p == rel_p_m)) {
-      double k1 = q[Q_B1] / (q[Q_LEN] * rel_p);
-      mx = quad_mat2_calc(-k1, step, rel_p);
-      my = quad_mat2_calc(k1, step, rel_p);
+      const int cls = R.h->aux0;
+      double* c = qm.q + (cls * 13) * qm.stride;
+      if (cls >= 0 && c[12 * qm.stride] == rel_p) {
+        mx = {c[0], c[qm.stride], c[2 * qm.stride], c[3 * qm.stride], c[4 * qm.stride], c[5 * qm.stride]};
+        my = {c[6 * qm.stride], c[7 * qm.stride], c[8 * qm.stride], c[9 * qm.stride], c[10 * qm.stride],
+              c[11 * qm.stride]};
+      } else {
+        double k1 = q[Q_B1] / (q[Q_LEN] * rel_p);
+        mx = quad_mat2_calc(-k1, step, rel_p);
+        my = quad_mat2_calc(k1, step, rel_p);
+        if (cls >= 0) {
+          const double v[12] = {mx.cx, mx.m01, mx.m10, mx.z0, mx.z1, mx.z2,
+                                my.cx, my.m01, my.m10, my.z0, my.z1, my.z2};
+#pragma unroll
+          for (int j = 0; j < 12; j++) c[j * qm.stride] = v[j];
+          c[12 * qm.stride] = rel_p;
+        }
+      }
       rel_p_m = rel_p;
     }
     double x = p.x, px = p.px, y = p.y, py = p.py;
@@ -428,7 +456,7 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
 // track1, bmad/code/track1.f90:43-342 for one alive particle and one record:
 // entrance aperture, body, orbit_too_large, exit aperture.  Returns the
 // particle's state (ALIVE or a lost code).
-__device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glob& G, DriftMemo& m) {
+__device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glob& G, DriftMemo& m, QMemo qm) {
   Rec R = decode(rec);
   const int32_t fl = R.h->flags;
   if ((fl & F_AP_ENTRANCE) && G.ap_on) {
@@ -440,7 +468,7 @@ __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glo
       track_a_drift<true>(p, R.kb[DR_L], G, m);
       break;
     case K_QUAD:
-      body_quad(p, R, G, m);
+      body_quad(p, R, G, m, qm);
       break;
     case K_BEND:
       body_bend(p, R, G, m);
@@ -514,11 +542,12 @@ struct KArgs {
   int64_t n_slots;               // slots (multiple of block size when tile_variant is set)
   // tables
   const double* tables;           // all variants, each 16-byte aligned
+  // Per variant: [sequence: n_rec x (int32 record offset in doubles, int32
+  // ix_ele)] [pool of unique records].  Identical elements share one record.
   const int64_t* table_off_dw;    // [variant] offset in doubles
   int32_t table_dw;               // doubles per table (max over variants, multiple of 2)
-  int32_t rec_begin, rec_end;     // record index range [begin, end) per turn
-  const int32_t* rec_off;         // [variant][record] offset in doubles within the table
-  int32_t n_rec;                  // records per table
+  int32_t rec_begin, rec_end;     // element range [begin, end) per turn
+  int32_t n_rec;                  // elements per table
   int32_t turn0, n_turns;
   int32_t compact_every;
   int32_t* tile_counter;
@@ -528,8 +557,8 @@ struct KArgs {
 
 constexpr int MAX_BLOCK = 256;
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) track_kernel(KArgs a) {
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
   extern __shared__ __align__(128) double smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t s_tile;
@@ -538,6 +567,9 @@ __global__ void __launch_bounds__(BLOCK) track_kernel(KArgs a) {
   // compaction staging area sits after the table
   double* stage = smem + a.table_dw;  // [9][BLOCK] doubles; rows 7-8 hold int32 ids and loss records
   int32_t* stage_i = reinterpret_cast<int32_t*>(stage + 7 * BLOCK);  // [3][BLOCK]
+  // quad memo after the (optional) compaction stage
+  double* qmemo_base = stage + (a.compact_every > 0 ? 9 * BLOCK : 0);
+  const QMemo qmemo{qmemo_base + threadIdx.x, BLOCK};
 
   const int tid = threadIdx.x;
   if (tid == 0) mbar_init(&bar, 1);
@@ -567,7 +599,7 @@ __global__ void __launch_bounds__(BLOCK) track_kernel(KArgs a) {
       parity ^= 1u;
       loaded_variant = variant;
     }
-    const int32_t* roff = a.rec_off + (int64_t)variant * a.n_rec;
+    const int2* seq = reinterpret_cast<const int2*>(table);
 
     // ---- load my particle ----
     const int64_t slot = tile * BLOCK + tid;
@@ -592,14 +624,15 @@ __global__ void __launch_bounds__(BLOCK) track_kernel(KArgs a) {
     DriftMemo memo;
     memo.pz = NAN;
     memo.a = 0;
+#pragma unroll
+    for (int c = 0; c < QMEMO_CLASSES; c++) qmemo.q[(c * 13 + 12) * qmemo.stride] = NAN;
     int32_t my_idx = (int32_t)pidx;  // particle carried by this lane (changes on compaction)
 
     // entrance check of the first element (check_aperture_limit ->
     // orbit_too_large, track1.f90:195)
     if (p.state == ALIVE) {
       if (orbit_too_large(p, a.G)) {
-        const RecHdr* h0 = reinterpret_cast<const RecHdr*>(table + roff[a.rec_begin]);
-        ixe = h0->ix_ele;
+        ixe = seq[a.rec_begin].y;
         ixt = a.turn0;
       }
     }
@@ -610,12 +643,12 @@ __global__ void __launch_bounds__(BLOCK) track_kernel(KArgs a) {
         // whole warp dead: nothing to do this turn (no block barrier inside
         // the turn unless compaction is on)
       } else {
-        const double* rec = table + roff[a.rec_begin];
-        for (int r = a.rec_begin; r < a.rec_end; r++, rec += reinterpret_cast<const RecHdr*>(rec)->size_dw) {
+        for (int r = a.rec_begin; r < a.rec_end; r++) {
+          const int2 e = seq[r];
           if (p.state == ALIVE) {
-            track1_rec(p, rec, a.G, memo);
+            track1_rec(p, table + e.x, a.G, memo, qmemo);
             if (p.state != ALIVE) {
-              ixe = reinterpret_cast<const RecHdr*>(rec)->ix_ele;
+              ixe = e.y;
               ixt = turn;
             }
           }
@@ -677,6 +710,8 @@ __global__ void __launch_bounds__(BLOCK) track_kernel(KArgs a) {
             ixt = stage_i[2 * BLOCK + tid];
             p.state = ALIVE;
             memo.pz = NAN;
+#pragma unroll
+            for (int c = 0; c < QMEMO_CLASSES; c++) qmemo.q[(c * 13 + 12) * qmemo.stride] = NAN;
           } else {
             p.state = 0;
             my_idx = -1;
@@ -1213,10 +1248,8 @@ struct bgt_handle {
   int32_t table_dw = 0;
   std::vector<double> h_tables;
   std::vector<int64_t> h_table_off;
-  std::vector<int32_t> h_rec_off;
   double* d_tables = nullptr;
   int64_t* d_table_off = nullptr;
-  int32_t* d_rec_off = nullptr;
   int32_t* d_scratch = nullptr;  // [0] tile counter, [1] error flag
   bgt_tuning tuning{128, 4, 0, 0};
   std::string err;
@@ -1243,19 +1276,20 @@ static int set_err(bgt_handle* h, int code, const std::string& msg) {
 static size_t smem_bytes(const bgt_handle* h, int block, bool compact) {
   size_t b = (size_t)h->table_dw * 8;
   if (compact) b += (size_t)9 * block * 8;
+  b += (size_t)QMEMO_CLASSES * 13 * block * 8;
   return b;
 }
 
-template <int BLOCK>
+template <int BLOCK, int MINB>
 static cudaError_t launch_track(const KArgs& a, int grid, size_t smem, cudaStream_t st) {
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          200 * 1024);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  track_kernel<BLOCK><<<grid, BLOCK, smem, st>>>(a);
+  track_kernel<BLOCK, MINB><<<grid, BLOCK, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1272,11 +1306,25 @@ static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t s
   a.error_flag = h->d_scratch + 1;
   CU(h, cudaMemsetAsync(h->d_scratch, 0, sizeof(int32_t), st));
   cudaError_t e;
-  switch (block) {
-    case 64: e = launch_track<64>(a, (int)grid, smem, st); break;
-    case 128: e = launch_track<128>(a, (int)grid, smem, st); break;
-    case 256: e = launch_track<256>(a, (int)grid, smem, st); break;
-    default: return set_err(h, BGT_EINVAL, "threads_per_block must be 64, 128 or 256");
+  // (threads per CTA, resident CTAs per SM) pairs compiled with matching
+  // __launch_bounds__, i.e. register caps of 128, 102, 85 and 64 per thread
+  const int bps = h->tuning.blocks_per_sm;
+  switch (block * 100 + bps) {
+    case 6408: e = launch_track<64, 8>(a, (int)grid, smem, st); break;
+    case 6410: e = launch_track<64, 10>(a, (int)grid, smem, st); break;
+    case 6412: e = launch_track<64, 12>(a, (int)grid, smem, st); break;
+    case 6416: e = launch_track<64, 16>(a, (int)grid, smem, st); break;
+    case 12804: e = launch_track<128, 4>(a, (int)grid, smem, st); break;
+    case 12805: e = launch_track<128, 5>(a, (int)grid, smem, st); break;
+    case 12806: e = launch_track<128, 6>(a, (int)grid, smem, st); break;
+    case 12808: e = launch_track<128, 8>(a, (int)grid, smem, st); break;
+    case 25602: e = launch_track<256, 2>(a, (int)grid, smem, st); break;
+    case 25603: e = launch_track<256, 3>(a, (int)grid, smem, st); break;
+    case 25604: e = launch_track<256, 4>(a, (int)grid, smem, st); break;
+    default:
+      return set_err(h, BGT_EINVAL,
+                     "tuning (threads_per_block, blocks_per_sm) must be one of (64: 8,10,12,16), "
+                     "(128: 4,5,6,8), (256: 2,3,4)");
   }
   if (e != cudaSuccess) return set_err(h, BGT_ECUDA, std::string("track_kernel launch: ") + cudaGetErrorString(e));
   h->launches++;
@@ -1288,7 +1336,6 @@ static KArgs base_args(bgt_handle* h) {
   a.tables = h->d_tables;
   a.table_off_dw = h->d_table_off;
   a.table_dw = h->table_dw;
-  a.rec_off = h->d_rec_off;
   a.n_rec = h->n_ele;
   a.rec_begin = 0;
   a.rec_end = h->n_ele;
@@ -1317,11 +1364,14 @@ int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t
   h->G.charge = species->charge;
   // compile tables
   std::vector<double> all;
+  const int32_t seq_dw = n_ele + (n_ele % 2);  // (offset, ix_ele) int32 pairs, padded to 16 bytes
   for (int v = 0; v < n_variants; v++) {
-    std::vector<double> tab;
+    std::vector<double> tab(seq_dw, 0.0);
+    std::unordered_map<std::string, int32_t> pool;  // record bytes -> offset (identical elements share)
+    std::unordered_map<std::string, int32_t> qclass;  // quad (length, b1, step) -> memo class
     for (int e = 0; e < n_ele; e++) {
-      h->h_rec_off.push_back((int32_t)tab.size());
-      int rc = host::compile_element(eles[(int64_t)v * n_ele + e], *species, p0c, tab, h->err);
+      std::vector<double> rec;
+      int rc = host::compile_element(eles[(int64_t)v * n_ele + e], *species, p0c, rec, h->err);
       if (rc) {
         std::string m = h->err;
         delete h;
@@ -1329,6 +1379,36 @@ int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t
         fprintf(stderr, "bgt_create: %s\n", m.c_str());
         return rc;
       }
+      RecHdr* rh = reinterpret_cast<RecHdr*>(rec.data());
+      rh->ix_ele = 0;  // carried by the sequence instead
+      if (rh->kind == K_QUAD) {
+        // quad-matrix memo class: same (b1, length, step) -> same quad_mat2_calc
+        const double* kb = rec.data() + HDR_DW + ((rh->flags & F_MISALIGN) ? MIS_N : 0) +
+                           ((rh->flags & (F_AP_ENTRANCE | F_AP_EXIT)) ? AP_N : 0);
+        std::string ck(reinterpret_cast<const char*>(kb), 3 * sizeof(double));  // Q_LEN, Q_B1, Q_STEP
+        auto ci = qclass.find(ck);
+        if (ci != qclass.end()) {
+          rh->aux0 = ci->second;
+        } else if ((int)qclass.size() < QMEMO_CLASSES) {
+          rh->aux0 = (int32_t)qclass.size();
+          qclass.emplace(ck, rh->aux0);
+        } else {
+          rh->aux0 = -1;
+        }
+      }
+      std::string key(reinterpret_cast<const char*>(rec.data()), rec.size() * sizeof(double));
+      auto it = pool.find(key);
+      int32_t off;
+      if (it != pool.end()) {
+        off = it->second;
+      } else {
+        off = (int32_t)tab.size();
+        tab.insert(tab.end(), rec.begin(), rec.end());
+        pool.emplace(std::move(key), off);
+      }
+      int32_t* s = reinterpret_cast<int32_t*>(tab.data()) + 2 * e;
+      s[0] = off;
+      s[1] = eles[(int64_t)v * n_ele + e].ix_ele;
     }
     h->table_dw = std::max(h->table_dw, (int32_t)tab.size());
     h->h_table_off.push_back((int64_t)all.size());
@@ -1344,12 +1424,9 @@ int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t
       (e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
       (e = cudaMalloc(&h->d_tables, all.size() * 8)) != cudaSuccess ||
       (e = cudaMalloc(&h->d_table_off, h->h_table_off.size() * 8)) != cudaSuccess ||
-      (e = cudaMalloc(&h->d_rec_off, h->h_rec_off.size() * 4)) != cudaSuccess ||
       (e = cudaMalloc(&h->d_scratch, 64)) != cudaSuccess ||
       (e = cudaMemcpy(h->d_tables, all.data(), all.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(h->d_table_off, h->h_table_off.data(), h->h_table_off.size() * 8, cudaMemcpyHostToDevice)) !=
-          cudaSuccess ||
-      (e = cudaMemcpy(h->d_rec_off, h->h_rec_off.data(), h->h_rec_off.size() * 4, cudaMemcpyHostToDevice)) !=
           cudaSuccess ||
       (e = cudaMemset(h->d_scratch, 0, 64)) != cudaSuccess) {
     fprintf(stderr, "bgt_create: CUDA error: %s\n", cudaGetErrorString(e));
@@ -1372,7 +1449,7 @@ int bgt_destroy(bgt_handle* h) {
   if (!h) return 0;
   cudaFree(h->d_tables);
   cudaFree(h->d_table_off);
-  cudaFree(h->d_rec_off);
+
   cudaFree(h->d_scratch);
   cudaFree(h->d_vec6);
   cudaFree(h->d_beta);
