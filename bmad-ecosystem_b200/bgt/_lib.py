@@ -53,7 +53,7 @@ _lib = None
 EXPORTED = [
     "bgt_create", "bgt_destroy", "bgt_last_error", "bgt_table_info", "bgt_set_tuning", "bgt_get_tuning",
     "bgt_track_turns", "bgt_track_turns_device", "bgt_track_elements", "bgt_da_scan_grid",
-    "bgt_kernel_launch_count", "bgt_fp64_peak_tflops",
+    "bgt_kernel_launch_count", "bgt_fp64_peak_tflops", "bgt_track_turns_device_noalloc",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -87,6 +87,10 @@ def load() -> C.CDLL:
     lib.bgt_kernel_launch_count.argtypes = [C.c_void_p]
     lib.bgt_kernel_launch_count.restype = C.c_int64
     lib.bgt_fp64_peak_tflops.argtypes = [C.c_int32, _dp]
+    lib.bgt_track_turns_device_noalloc.argtypes = [
+        C.POINTER(BgtElement), C.c_int32, C.POINTER(BgtSpecies), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+        C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.POINTER(BgtTuning), C.c_int32, C.c_void_p, C.c_char_p,
+        C.c_int32]
     _lib = lib
     return lib
 

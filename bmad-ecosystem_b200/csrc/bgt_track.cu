@@ -1848,3 +1848,166 @@ int bgt_fp64_peak_tflops(int32_t device, double* tflops) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free tracking entry point.
+//
+// For callers that cannot allocate device memory from inside this library:
+// hosts whose framework owns the device memory (a caching allocator that has
+// reserved the GPU, so a cudaMalloc here could fail or fragment its pool) and
+// loops that must not allocate per call.  The element table, the tile
+// counter and the error flag live in one file-scope device array instead of
+// handle-owned cudaMalloc buffers; the caller passes the particle arrays.
+//
+// The array holds BGT_NOALLOC_SCRATCH_BYTES on every GPU that loads this
+// library, until the process exits.  Tables larger than that are rejected.
+// Every call uses the same array and leaves its contents behind: calls that
+// overlap on the GPU (different streams, or threads) race and must be
+// serialised by the caller.  The first call on a device resolves the array's
+// address (cudaGetSymbolAddress) and uploads the multipole coefficient
+// tables; make that first call before any stream capture.
+
+#define BGT_NOALLOC_SCRATCH_BYTES (256 * 1024)
+
+namespace bgt {
+
+// [0..15]: tile counter (int32), error flag (int32); table from byte 256 on
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BGT_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};
+}  // namespace
+
+}  // namespace bgt
+
+extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n_ele, const bgt_species* species,
+                                              double* d_vec6, double* d_beta, int32_t* d_state,
+                                              int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, int64_t n,
+                                              int32_t turn0, int32_t n_turns, const bgt_tuning* tuning,
+                                              int32_t device, void* stream, char* err, int32_t err_len) {
+  auto fail = [&](int code, const std::string& msg) {
+    if (err && err_len > 0) {
+      snprintf(err, (size_t)err_len, "%s", msg.c_str());
+    }
+    return code;
+  };
+  if (!eles || !species || n_ele <= 0 || !d_vec6 || !d_beta || !d_state || !d_ix_ele_lost || n < 0 ||
+      n_turns < 0 || device < 0 || device >= bgt::kNoallocMaxDevices)
+    return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: invalid argument");
+  if (n == 0 || n_turns == 0) return 0;
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
+
+  // one-time set-up on this device (this device current)
+  if (!bgt::g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    ce = cudaGetSymbolAddress(&p, bgt::g_noalloc_scratch);
+    if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+    static double cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1], cm0[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
+    bgt::host::c_multi_tables(cm, cm0);
+    if ((ce = cudaMemcpyToSymbol(bgt::c_cm, cm, sizeof(cm))) != cudaSuccess ||
+        (ce = cudaMemcpyToSymbol(bgt::c_cm0, cm0, sizeof(cm0))) != cudaSuccess)
+      return fail(BGT_ECUDA, std::string("coefficient upload: ") + cudaGetErrorString(ce));
+    bgt::g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  unsigned char* base = bgt::g_noalloc_ptr[device];
+
+  // compile the table on the host (same records as bgt_create, one variant)
+  std::vector<double> tab((size_t)(n_ele + (n_ele % 2)), 0.0);
+  std::unordered_map<std::string, int32_t> pool;
+  std::string msg;
+  const double p0c = eles[0].p0c;
+  for (int e = 0; e < n_ele; e++) {
+    std::vector<double> rec;
+    int rc = bgt::host::compile_element(eles[e], *species, p0c, rec, msg);
+    if (rc) return fail(rc, msg);
+    bgt::RecHdr* rh = reinterpret_cast<bgt::RecHdr*>(rec.data());
+    rh->ix_ele = 0;
+    if (rh->kind == bgt::K_QUAD) rh->aux0 = -1;  // no quad memo classes on this path
+    std::string key(reinterpret_cast<const char*>(rec.data()), rec.size() * sizeof(double));
+    auto it = pool.find(key);
+    int32_t off;
+    if (it != pool.end()) {
+      off = it->second;
+    } else {
+      off = (int32_t)tab.size();
+      tab.insert(tab.end(), rec.begin(), rec.end());
+      pool.emplace(std::move(key), off);
+    }
+    int32_t* s = reinterpret_cast<int32_t*>(tab.data()) + 2 * e;
+    s[0] = off;
+    s[1] = eles[e].ix_ele;
+  }
+  if (tab.size() % 2) tab.push_back(0.0);
+  const size_t table_bytes = tab.size() * sizeof(double);
+  if (256 + table_bytes > BGT_NOALLOC_SCRATCH_BYTES)
+    return fail(BGT_ETOOLARGE, "bgt_track_turns_device_noalloc: element table needs " +
+                                   std::to_string(table_bytes) + " bytes, the scratch array holds " +
+                                   std::to_string(BGT_NOALLOC_SCRATCH_BYTES - 256));
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t* d_counter = reinterpret_cast<int32_t*>(base);
+  double* d_table = reinterpret_cast<double*>(base + 256);
+  // table offset 0 for the single variant, kept in the scratch header
+  int64_t* d_table_off = reinterpret_cast<int64_t*>(base + 16);
+  const int64_t zero_off = 0;
+  if ((ce = cudaMemcpyAsync(d_table, tab.data(), table_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (ce = cudaMemcpyAsync(d_table_off, &zero_off, sizeof(zero_off), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return fail(BGT_ECUDA, std::string("table upload: ") + cudaGetErrorString(ce));
+
+  bgt_tuning t = tuning ? *tuning : bgt_tuning{128, 4, 0, 0};
+  if (t.threads_per_block == 0) t.threads_per_block = 128;
+  if (t.blocks_per_sm == 0) t.blocks_per_sm = 4;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+
+  bgt::KArgs a{};
+  a.vec6 = d_vec6;
+  a.beta = d_beta;
+  a.state = d_state;
+  a.ix_ele_lost = d_ix_ele_lost;
+  a.ix_turn_lost = d_ix_turn_lost;
+  a.n = n;
+  a.n_stride = n;
+  a.n_slots = n;
+  a.tables = d_table;
+  a.table_off_dw = d_table_off;
+  a.table_dw = (int32_t)tab.size();
+  a.rec_begin = 0;
+  a.rec_end = n_ele;
+  a.n_rec = n_ele;
+  a.compact_every = t.compact_every;
+  a.tile_counter = d_counter;
+  a.error_flag = d_counter + 1;
+  a.G.mc2 = species->mass;
+  a.G.mc2sq = species->mass * species->mass;
+  a.G.p0c = p0c;
+  a.G.mal = species->max_aperture_limit;
+  a.G.ap_on = species->aperture_limit_on;
+  a.G.charge = species->charge;
+  const int block = t.threads_per_block;
+  size_t smem = (size_t)a.table_dw * 8 + (t.compact_every > 0 ? (size_t)9 * block * 8 : 0) +
+                (size_t)bgt::QMEMO_CLASSES * 13 * block * 8;
+  if (smem > 200 * 1024) return fail(BGT_ETOOLARGE, "element table does not fit in shared memory");
+  const int64_t n_tiles = (n + block - 1) / block;
+  int64_t grid = std::min<int64_t>((int64_t)sms * t.blocks_per_sm, n_tiles);
+  if (grid < 1) grid = 1;
+  // the counter and error flag must start at zero for every launch
+  if ((ce = cudaMemsetAsync(d_counter, 0, 2 * sizeof(int32_t), st)) != cudaSuccess)
+    return fail(BGT_ECUDA, std::string("scratch clear: ") + cudaGetErrorString(ce));
+  const int32_t seg = t.turns_per_launch > 0 ? t.turns_per_launch : n_turns;
+  for (int32_t k = 0; k < n_turns; k += seg) {
+    a.turn0 = turn0 + k;
+    a.n_turns = std::min(seg, n_turns - k);
+    if (k > 0 && (ce = cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st)) != cudaSuccess)
+      return fail(BGT_ECUDA, std::string("scratch clear: ") + cudaGetErrorString(ce));
+    switch (block * 100 + t.blocks_per_sm) {
+      case 12804: ce = launch_track<128, 4>(a, (int)grid, smem, st); break;
+      case 25602: ce = launch_track<256, 2>(a, (int)grid, smem, st); break;
+      default:
+        return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: tuning must be (128, 4) or (256, 2)");
+    }
+    if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("track_kernel launch: ") + cudaGetErrorString(ce));
+  }
+  return 0;
+}

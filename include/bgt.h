@@ -211,6 +211,31 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
 /* Number of this library's kernels launched since the handle was created. */
 int64_t bgt_kernel_launch_count(const bgt_handle* h);
 
+/*
+ * Allocation-free variant of bgt_track_turns_device (no counterpart in the
+ * reference).  For callers that cannot let this library allocate device
+ * memory: hosts whose framework owns the GPU's memory through its own
+ * caching allocator, and loops that must not allocate per call.  It needs no
+ * handle: it compiles the n_ele elements (one lattice) on the host, copies
+ * the table into a fixed device array inside the library, and tracks the
+ * caller's device particle arrays in place on `stream`.  It never calls
+ * cudaMalloc or cudaFree.
+ *
+ * Limits: the array holds 256 KiB (table plus a 256-byte header) on every
+ * GPU that loads the library, until the process exits; larger tables are
+ * rejected with BGT_ETOOLARGE.  Every call reuses the same array and leaves
+ * its contents behind, so calls that overlap on the GPU (other streams or
+ * threads) race: serialise them.  The first call on a device looks up the
+ * array's address and uploads constant tables; make it before any stream
+ * capture.  tuning may be NULL; otherwise (threads, CTAs per SM) must be
+ * (128, 4) or (256, 2).  On error a message is written to err (err_len bytes).
+ */
+int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n_ele, const bgt_species* species,
+                                   double* d_vec6, double* d_beta, int32_t* d_state, int32_t* d_ix_ele_lost,
+                                   int32_t* d_ix_turn_lost, int64_t n, int32_t turn0, int32_t n_turns,
+                                   const bgt_tuning* tuning, int32_t device, void* stream, char* err,
+                                   int32_t err_len);
+
 /* Measured FP64 FMA throughput of `device` in TFLOP/s (2 flops per FMA):
  * the roofline denominator for the tracking kernel.  No reference
  * counterpart (measurement helper). */
