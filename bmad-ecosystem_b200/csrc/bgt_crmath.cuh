@@ -105,6 +105,54 @@ BGT_HD bool round_test(dd v, double err, double* out) {
   return false;
 }
 
+// ---- light fast paths for small arguments, 2^-27 <= |x| <= 2^-4 ----
+//
+// Every particle-dependent argument in a bend step (phi_1 = asin(px/pt),
+// angle + phi_1, the atan2 ratio, the exit angle) and the per-step focusing
+// phase of a quadrupole is a few 1e-2 or smaller, where one plain-double
+// polynomial already lands within a few thousandths of an ulp.  u = 2^-53.
+//
+// Odd series  f(x) = x + x y P(y),  y = fl(x^2),
+//             P(y) = C[1] + C[2] y + ... + C[K] y^(K-1)  (Horner, plain double).
+//   |x y P| <= |x| y / 3 <= 1.3e-3 |x|.  Relative error of the computed
+//   correction c: y (u), x*y (u), P (2u + O(u y): the C[1] rounding and the
+//   final add dominate), the product (u) -> < 6.1u < 8u = 2^-50.  The
+//   omitted terms are < 2^-70 |x| for the K used (sin/sinh K=5: < y^6/13!;
+//   asin K=8: < 0.0098 y^9; atan K=8: < y^9/19), and 2^-69 |x| also covers
+//   the roundings inside round_test.  hi + lo = x + c exactly (|x| >= |c|).
+// Even series f(x) = 1 + C[1] y + y^2 Q(y), C[1] = -1/2 (cos) or 1/2 (cosh)
+//   is a power of two, so C[1] (yh + yl) with yh + yl = x^2 (two_prod) is
+//   exact; t = yh^2 Q(yh) carries < 6u relative error; the two roundings
+//   in the low word are < |t| 2^-53 + 2^-105; omitted terms < y^6/12! < 2^-77.
+//
+// Below 2^-27, |x|^3/6 (asin, sinh: x^3/6; atan: x^3/3) is below half an ulp
+// of x and x^2/2 below half an ulp of 1, so the correctly rounded value is
+// x (odd) or 1 (even); that also keeps every product here normal.
+template <int K>
+BGT_HD bool odd_series_light(double x, const double (*C)[2], double* out) {
+  double y = x * x;
+  double p = C[K][0];
+#pragma unroll
+  for (int k = K - 1; k >= 1; k--) p = p * y + C[k][0];
+  double c = (x * y) * p;
+  dd s = fast_two_sum(x, c);
+  double err = fabs(c) * 0x1p-50 + fabs(x) * 0x1p-69;
+  return round_test(s, err, out);
+}
+
+template <int K>
+BGT_HD bool even_series_light(double x, const double (*C)[2], double* out) {
+  dd y = two_prod(x, x);
+  double q = C[K][0];
+#pragma unroll
+  for (int k = K - 1; k >= 2; k--) q = q * y.hi + C[k][0];
+  double t = (y.hi * y.hi) * q;
+  dd s = fast_two_sum(1.0, y.hi * C[1][0]);
+  s.lo = s.lo + (y.lo * C[1][0] + t);
+  double err = fabs(t) * 0x1p-49 + 0x1p-100;
+  return round_test(s, err, out);
+}
+
 // ---- double-double Taylor kernels on a reduced double-double argument ----
 
 // sin(r), |r| <= pi/4 + tiny
@@ -194,6 +242,11 @@ BGT_HD double cos_fast_or_nan(double x) {
 BGT_HD double sin(double x) {
   if (!(fabs(x) < 524288.0)) return ::sin(x);  // non-finite or huge: library value
   if (x == 0) return x;
+  if (fabs(x) <= 0x1p-4) {
+    if (fabs(x) < 0x1p-27) return x;
+    double f;
+    if (odd_series_light<5>(x, SIN_C, &f)) return f;
+  }
   if (fabs(x) <= 0.78539816339744828) {
     double f = sin_fast_or_nan(x);
     if (f == f) return f;
@@ -205,6 +258,11 @@ BGT_HD double sin(double x) {
 
 BGT_HD double cos(double x) {
   if (!(fabs(x) < 524288.0)) return ::cos(x);
+  if (fabs(x) <= 0x1p-4) {
+    if (fabs(x) < 0x1p-27) return 1.0;
+    double f;
+    if (even_series_light<5>(x, COS_C, &f)) return f;
+  }
   if (fabs(x) <= 0.78539816339744828) {
     double f = cos_fast_or_nan(x);
     if (f == f) return f;
@@ -240,6 +298,11 @@ BGT_HD double sinh(double x) {
   double a = fabs(x);
   if (!(a <= 2.0)) return ::sinh(x);
   if (x == 0) return x;
+  if (a <= 0x1p-4) {
+    if (a < 0x1p-27) return x;
+    double f;
+    if (odd_series_light<5>(x, SINH_C, &f)) return f;
+  }
   if (a <= 0.78539816339744828) {
     dd x2 = two_prod(x, x);
     dd x3 = dd_mul_d(x2, x);
@@ -264,6 +327,11 @@ BGT_HD double sinh(double x) {
 BGT_HD double cosh(double x) {
   double a = fabs(x);
   if (!(a <= 2.0)) return ::cosh(x);
+  if (a <= 0x1p-4) {
+    if (a < 0x1p-27) return 1.0;
+    double f;
+    if (even_series_light<5>(x, COSH_C, &f)) return f;
+  }
   if (a <= 0.78539816339744828) {
     dd x2 = two_prod(x, x);
     dd x4 = dd_mul(x2, x2);
@@ -299,6 +367,11 @@ BGT_HD double asin(double u) {
   double a = fabs(u);
   if (!(a <= 1.0)) return ::asin(u);  // |u| > 1 or NaN
   if (u == 0) return u;
+  if (a <= 0x1p-4) {
+    if (a < 0x1p-27) return u;
+    double f;
+    if (odd_series_light<8>(u, ASIN_C, &f)) return f;
+  }
   if (a <= 0.125) {
     dd u2 = two_prod(u, u);
     dd u3 = dd_mul_d(u2, u);
@@ -359,6 +432,21 @@ BGT_HD double atan2(double y, double x) {
   // q = y / x as double-double (exact remainder by fma)
   double qh = y / x;
   double ql = fma(-qh, x, y) / x;
+  if (x > 0 && fabs(qh) <= 0x1p-4) {
+    // atan(qh + ql) = atan(qh) + ql - ql qh^2 / (1 + qh^2) + O(ql^2): the
+    // odd-series bound for atan(qh) (K = 8) plus the rounding of c + ql,
+    // the error of ql (u) and the dropped ql qh^2 term (< 2 |ql| yy).
+    double yy = qh * qh;
+    double p = ATAN_C[8][0];
+#pragma unroll
+    for (int k = 7; k >= 1; k--) p = p * yy + ATAN_C[k][0];
+    double c = (qh * yy) * p;
+    double t = c + ql;
+    dd s = fast_two_sum(qh, t);
+    double err = fabs(c) * 0x1p-50 + fabs(t) * 0x1p-52 + fabs(ql) * (2 * yy + 0x1p-52) + fabs(qh) * 0x1p-69;
+    double out;
+    if (round_test(s, err, &out)) return out;
+  }
   if (x > 0 && fabs(qh) <= 0.125) {
     dd q2 = two_prod(qh, qh);
     dd q3 = dd_mul_d(q2, qh);

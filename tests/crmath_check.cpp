@@ -1,0 +1,93 @@
+// Host check of the device's correctly rounded sin/cos/sinh/cosh/asin/atan2
+// (bmad-ecosystem_b200/csrc/bgt_crmath.cuh, compiled here for the CPU)
+// against libquadmath evaluated in binary128 and rounded to double.
+//
+// usage: crmath_check <samples per range> <seed>
+// prints one line per (function, range): "<fn> <lo> <hi> <mismatches> <samples>"
+// and the first few mismatches as "MISMATCH ..." lines.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <quadmath.h>
+
+#include "../bmad-ecosystem_b200/csrc/bgt_crmath.cuh"
+
+static uint64_t S;
+static double uni() {  // [0, 1)
+  S ^= S << 13;
+  S ^= S >> 7;
+  S ^= S << 17;
+  return (S >> 11) * (1.0 / 9007199254740992.0);
+}
+// uniform in [lo, hi] (mode 0) or sign * 2^uniform(log2 lo, log2 hi) (mode 1)
+static double draw(double lo, double hi, int mode) {
+  if (mode == 0) return lo + (hi - lo) * uni();
+  double e = std::log2(lo) + (std::log2(hi) - std::log2(lo)) * uni();
+  double v = std::exp2(e);
+  return (uni() < 0.5) ? -v : v;
+}
+
+struct Range {
+  const char* fn;
+  double lo, hi;
+  int mode;
+};
+
+static double cr_eval(const char* fn, double x, double y) {
+  if (!strcmp(fn, "sin")) return bgt::cr::sin(x);
+  if (!strcmp(fn, "cos")) return bgt::cr::cos(x);
+  if (!strcmp(fn, "sinh")) return bgt::cr::sinh(x);
+  if (!strcmp(fn, "cosh")) return bgt::cr::cosh(x);
+  if (!strcmp(fn, "asin")) return bgt::cr::asin(x);
+  return bgt::cr::atan2(y, x);
+}
+static double q_eval(const char* fn, double x, double y) {
+  __float128 q;
+  if (!strcmp(fn, "sin")) q = sinq(x);
+  else if (!strcmp(fn, "cos")) q = cosq(x);
+  else if (!strcmp(fn, "sinh")) q = sinhq(x);
+  else if (!strcmp(fn, "cosh")) q = coshq(x);
+  else if (!strcmp(fn, "asin")) q = asinq(x);
+  else q = atan2q(y, x);
+  return (double)q;
+}
+
+int main(int argc, char** argv) {
+  long n = argc > 1 ? atol(argv[1]) : 100000;
+  S = argc > 2 ? strtoull(argv[2], nullptr, 10) : 88172645463325252ULL;
+  if (S == 0) S = 1;
+  const Range rs[] = {
+      // light paths (2^-27 .. 2^-4) and their edges
+      {"sin", 0x1p-30, 0x1p-4, 1}, {"sin", -0.0625, 0.0625, 0}, {"sin", 0.0155, 0.0175, 0},
+      {"cos", 0x1p-30, 0x1p-4, 1}, {"cos", -0.0625, 0.0625, 0},
+      {"sinh", 0x1p-30, 0x1p-4, 1}, {"cosh", 0x1p-30, 0x1p-4, 1},
+      {"asin", 0x1p-30, 0x1p-4, 1}, {"asin", -2e-3, 2e-3, 0},
+      {"atan2", 0x1p-30, 0x1p-4, 1}, {"atan2", -0.0625, 0.0625, 0},
+      // double-double fast paths and the slow paths behind them
+      {"sin", -0.78, 0.78, 0}, {"sin", -30.0, 30.0, 0}, {"cos", -0.78, 0.78, 0}, {"cos", -30.0, 30.0, 0},
+      {"sinh", -2.0, 2.0, 0}, {"cosh", -2.0, 2.0, 0}, {"asin", -1.0, 1.0, 0}, {"atan2", -4.0, 4.0, 0},
+  };
+  long total_bad = 0;
+  for (const Range& r : rs) {
+    long bad = 0;
+    for (long i = 0; i < n; i++) {
+      double x = draw(r.lo, r.hi, r.mode), y = 0;
+      if (!strcmp(r.fn, "atan2")) {
+        // ratio q = x; denominator a positive (mostly) scale, as in the bend map
+        double den = (i % 8 == 7) ? -(0.25 + 2 * uni()) : (0.25 + 2 * uni());
+        y = x * den;
+        x = den;
+      }
+      double c = cr_eval(r.fn, x, y), q = q_eval(r.fn, x, y);
+      if (c != q && !(std::isnan(c) && std::isnan(q))) {
+        if (bad < 3) printf("MISMATCH %s(%a, %a) cr=%a ref=%a\n", r.fn, x, y, c, q);
+        bad++;
+      }
+    }
+    total_bad += bad;
+    printf("%s %.17g %.17g %ld %ld\n", r.fn, r.lo, r.hi, bad, n);
+  }
+  return total_bad ? 1 : 0;
+}
