@@ -49,11 +49,15 @@ class BgtError(RuntimeError):
 
 _lib = None
 
-# every symbol include/bgt.h declares
+# every symbol include/bgt.h and include/bgt_mlp.h declare
 EXPORTED = [
     "bgt_create", "bgt_destroy", "bgt_last_error", "bgt_table_info", "bgt_set_tuning", "bgt_get_tuning",
     "bgt_track_turns", "bgt_track_turns_device", "bgt_track_elements", "bgt_da_scan_grid",
     "bgt_kernel_launch_count", "bgt_fp64_peak_tflops", "bgt_track_turns_device_noalloc",
+    # include/bgt_mlp.h
+    "bgt_mlp_create", "bgt_mlp_destroy", "bgt_mlp_last_error", "bgt_mlp_launch_count", "bgt_mlp_get_params",
+    "bgt_mlp_set_params", "bgt_mlp_forward", "bgt_mlp_gradients", "bgt_mlp_train_step", "bgt_mlp_features",
+    "bgt_mlp_gemm_bf16",
 ]
 
 _dp = C.POINTER(C.c_double)

@@ -154,22 +154,28 @@ class Tracker:
         return self.track_elements(bunch, position, position + 1, variant)
 
     def track_turns_device(self, vec6, beta, state, ix_ele_lost, ix_turn_lost, n_turns: int, turn0: int = 0,
-                           stream=None):
+                           stream=None, variant=None):
         """Track device-resident torch tensors in place, enqueued on `stream`
-        (a torch.cuda.Stream; default: the current stream)."""
+        (a torch.cuda.Stream; default: the current stream).  `variant` (int32
+        CUDA tensor, sorted) selects each particle's lattice variant; with
+        more than one variant the call synchronises the stream once."""
         import torch
 
         if stream is None:
             stream = torch.cuda.current_stream(vec6.device)
-        for t, dt in ((vec6, torch.float64), (beta, torch.float64), (state, torch.int32),
-                      (ix_ele_lost, torch.int32), (ix_turn_lost, torch.int32)):
+        checks = [(vec6, torch.float64), (beta, torch.float64), (state, torch.int32), (ix_ele_lost, torch.int32),
+                  (ix_turn_lost, torch.int32)]
+        if variant is not None:
+            checks.append((variant, torch.int32))
+        for t, dt in checks:
             if not t.is_cuda or t.dtype != dt or not t.is_contiguous():
                 raise ValueError("device tensors must be contiguous CUDA tensors of the documented dtype")
         n = beta.numel()
-        if vec6.numel() != 6 * n:
-            raise ValueError("vec6 must hold 6*n values")
+        if vec6.numel() != 6 * n or (variant is not None and variant.numel() != n):
+            raise ValueError("vec6 must hold 6*n values and variant n")
         rc = self.lib.bgt_track_turns_device(self.h, vec6.data_ptr(), beta.data_ptr(), state.data_ptr(),
-                                             ix_ele_lost.data_ptr(), ix_turn_lost.data_ptr(), None, n, turn0,
+                                             ix_ele_lost.data_ptr(), ix_turn_lost.data_ptr(),
+                                             variant.data_ptr() if variant is not None else None, n, turn0,
                                              n_turns, C.c_void_p(stream.cuda_stream))
         _check(self.lib, self.h, rc, "bgt_track_turns_device")
 

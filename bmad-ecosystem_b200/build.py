@@ -15,7 +15,7 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SRC = HERE / "csrc" / "bgt_track.cu"
+SRCS = [HERE / "csrc" / "bgt_track.cu", HERE / "csrc" / "bgt_mlp.cu"]
 OUT = HERE / "bgt" / "libbgt.so"
 
 
@@ -27,21 +27,34 @@ def nvcc() -> str:
 
 
 def build(fmad: bool = False, out: Path = OUT, verbose: bool = False) -> Path:
-    deps = list((HERE / "csrc").glob("*")) + [HERE.parent / "include" / "bgt.h"]
+    deps = list((HERE / "csrc").glob("*")) + list((HERE.parent / "include").glob("*.h"))
     if out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps) and not os.environ.get(
             "BGT_FORCE_BUILD"):
         return out
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-           f"--fmad={'true' if fmad else 'false'}", "-Xcompiler", "-fPIC", "-shared", "-o", str(out), str(SRC),
-           "-lquadmath"]
+    common = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              f"--fmad={'true' if fmad else 'false'}", "-Xcompiler", "-fPIC"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        common.insert(1, "-Xptxas=-v")
+    objdir = out.parent / "_obj"
+    objdir.mkdir(exist_ok=True)
+    objs = [objdir / (s.stem + ".o") for s in SRCS]
+    procs = [subprocess.Popen(common + ["-c", "-o", str(o), str(s)], stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                              text=True) for s, o in zip(SRCS, objs)]
+    errs = []
+    for p in procs:
+        so, se = p.communicate()
+        if p.returncode != 0:
+            errs.append(so + se)
+        elif verbose:
+            sys.stderr.write(se)
+    if errs:
+        sys.stderr.write("\n".join(errs))
+        raise RuntimeError("nvcc failed building libbgt.so")
+    r = subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(out)] +
+                       [str(o) for o in objs] + ["-lquadmath"], capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libbgt.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libbgt.so")
     return out
 
 

@@ -1259,6 +1259,11 @@ struct bgt_handle {
   double* d_beta = nullptr;
   int32_t* d_i32 = nullptr;  // state, ixe, ixt, slot map, tile variant
   int64_t cap = 0, cap_slots = 0, cap_tiles = 0;
+  // device-API grouping by variant: slot map, tile variant, and per variant
+  // first index / count / first slot (int64) plus a check flag
+  int32_t* d_grp = nullptr;
+  int64_t* d_grp_v = nullptr;
+  int64_t grp_cap_slots = 0, grp_cap_tiles = 0;
 };
 
 static int set_err(bgt_handle* h, int code, const std::string& msg) {
@@ -1454,6 +1459,8 @@ int bgt_destroy(bgt_handle* h) {
   cudaFree(h->d_vec6);
   cudaFree(h->d_beta);
   cudaFree(h->d_i32);
+  cudaFree(h->d_grp);
+  cudaFree(h->d_grp_v);
   delete h;
   return 0;
 }
@@ -1517,16 +1524,90 @@ static int track_device_impl(bgt_handle* h, double* d_vec6, int64_t n_stride, do
   return 0;
 }
 
+// Per-variant particle counts of a variant-sorted device array, with a check
+// that ids are in range (bad bit 1) and non-decreasing (bad bit 2).
+__global__ void variant_count_kernel(const int32_t* var, int64_t n, int32_t n_var, int64_t* first, int64_t* count,
+                                     int32_t* bad) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int32_t v = var[i];
+  if (v < 0 || v >= n_var) {
+    atomicOr(bad, 1);
+    return;
+  }
+  if (i > 0 && var[i - 1] > v) atomicOr(bad, 2);
+  if (i == 0 || var[i - 1] != v) first[v] = i;
+  atomicAdd((unsigned long long*)&count[v], 1ull);
+}
+
+// slot of particle i: its variant's first slot + its rank inside the variant
+__global__ void variant_slot_kernel(const int32_t* var, int64_t n, const int64_t* first, const int64_t* slot0,
+                                    int32_t* slot) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int32_t v = var[i];
+  slot[slot0[v] + (i - first[v])] = (int32_t)i;
+}
+
 int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state, int32_t* d_ix_ele_lost,
                            int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n, int32_t turn0,
                            int32_t n_turns, void* stream) {
   if (!h || !d_vec6 || !d_beta || !d_state || !d_ix_ele_lost || n < 0 || n_turns < 0) return BGT_EINVAL;
-  if (d_variant && h->n_variants > 1)
-    return set_err(h, BGT_EUNSUPPORTED, "bgt_track_turns_device: per-particle variants need bgt_track_turns");
   if (n == 0 || n_turns == 0) return 0;
+  if (n > INT32_MAX) return set_err(h, BGT_EINVAL, "bgt_track_turns_device: n exceeds 2^31 - 1");
   CU(h, cudaSetDevice(h->device));
-  return track_device_impl(h, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost, nullptr, nullptr, n, n,
-                           turn0, n_turns, 0, h->n_ele, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!d_variant || h->n_variants == 1)
+    return track_device_impl(h, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost, nullptr, nullptr, n, n,
+                             turn0, n_turns, 0, h->n_ele, st);
+  // Group by variant into tile-aligned slot ranges.  The variant ids must be
+  // sorted (non-decreasing); the per-variant counts are read back once.
+  const int32_t nv = h->n_variants;
+  const int block = h->tuning.threads_per_block;
+  if (!h->d_grp_v) CU(h, cudaMalloc(&h->d_grp_v, ((size_t)3 * nv + 1) * 8));
+  int64_t* d_first = h->d_grp_v;
+  int64_t* d_count = d_first + nv;
+  int64_t* d_slot0 = d_count + nv;
+  int32_t* d_bad = (int32_t*)(d_slot0 + nv);
+  CU(h, cudaMemsetAsync(d_first, 0, ((size_t)3 * nv + 1) * 8, st));
+  variant_count_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_variant, n, nv, d_first, d_count, d_bad);
+  h->launches++;
+  std::vector<int64_t> cnt((size_t)nv + 1);
+  CU(h, cudaMemcpyAsync(cnt.data(), d_count, (size_t)nv * 8, cudaMemcpyDeviceToHost, st));
+  int32_t bad = 0;
+  CU(h, cudaMemcpyAsync(&bad, d_bad, 4, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaStreamSynchronize(st));
+  if (bad & 1) return set_err(h, BGT_EINVAL, "bgt_track_turns_device: variant id out of range");
+  if (bad & 2) return set_err(h, BGT_EINVAL, "bgt_track_turns_device: variant ids must be sorted");
+  std::vector<int64_t> slot0(nv);
+  std::vector<int32_t> tvar;
+  int64_t s = 0;
+  for (int32_t v = 0; v < nv; v++) {
+    slot0[v] = s;
+    int64_t tiles = (cnt[v] + block - 1) / block;
+    for (int64_t t = 0; t < tiles; t++) tvar.push_back(v);
+    s += tiles * block;
+  }
+  const int64_t n_slots = s, n_tiles = (int64_t)tvar.size();
+  if (n_slots > h->grp_cap_slots || n_tiles > h->grp_cap_tiles) {
+    CU(h, cudaStreamSynchronize(st));
+    cudaFree(h->d_grp);
+    h->d_grp = nullptr;
+    h->grp_cap_slots = std::max(n_slots, h->grp_cap_slots);
+    h->grp_cap_tiles = std::max(n_tiles, h->grp_cap_tiles);
+    CU(h, cudaMalloc(&h->d_grp, (size_t)(h->grp_cap_slots + h->grp_cap_tiles) * 4));
+  }
+  int32_t* d_slot = h->d_grp;
+  int32_t* d_tvar = d_slot + h->grp_cap_slots;
+  CU(h, cudaMemcpyAsync(d_slot0, slot0.data(), (size_t)nv * 8, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemcpyAsync(d_tvar, tvar.data(), (size_t)n_tiles * 4, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemsetAsync(d_slot, 0xff, (size_t)n_slots * 4, st));
+  variant_slot_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_variant, n, d_first, d_slot0, d_slot);
+  h->launches++;
+  // (copies from pageable host memory return once the data is staged, so
+  // slot0 and tvar may go out of scope before the copies complete)
+  return track_device_impl(h, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost, d_slot, d_tvar, n, n_slots,
+                           turn0, n_turns, 0, h->n_ele, st);
 }
 
 // Grow the host-API staging buffers.

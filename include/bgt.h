@@ -178,6 +178,10 @@ int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, i
  * Same, DEVICE buffers already resident in HBM, enqueued on `stream`
  * (a cudaStream_t, NULL = legacy default stream).  Asynchronous.
  * Uses library-owned scratch sized on first use (grown as needed).
+ * d_variant (device int32[n], may be NULL = variant 0) must be sorted
+ * (non-decreasing); with it and more than one variant the call counts the
+ * particles per variant on the device and synchronises `stream` once to read
+ * the counts back (BGT_EINVAL for unsorted or out-of-range ids).
  */
 int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state,
                            int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n,

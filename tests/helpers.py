@@ -117,3 +117,56 @@ def oracle_track_elements(lat: L.Lattice, vec6: np.ndarray, start: int, stop: in
     it = np.full(n, -1, np.int32)
     O.track_turns(eles, lat.p0c, param, v, b, st, ie, it, n_turns, n_threads=threads, lib=lib)
     return v, b, st, ie, it
+
+
+def oracle_batch_one_turn(lattices, variant: str = "cr"):
+    """(vec6[6, m], variant[m]) -> vec6 after one turn, through the oracle,
+    each particle in its own variant's lattice."""
+    from oracle import oracle as O
+
+    lib = O.load(variant=variant)
+    eles = [O.to_eles(lat, lib) for lat in lattices]
+    lat0 = lattices[0]
+    param = O.make_param(lat0.species.mass, lat0.species.charge)
+
+    def f(vec6, var):
+        out = np.array(vec6, dtype=np.float64, copy=True)
+        for v in np.unique(var):
+            idx = np.nonzero(var == v)[0]
+            sub = np.ascontiguousarray(out[:, idx])
+            n = sub.shape[1]
+            beta = O.beta_of(lat0.p0c, sub[5], lat0.species.mass)
+            st = np.ones(n, np.int32)
+            ie = np.full(n, -1, np.int32)
+            it = np.full(n, -1, np.int32)
+            O.track_turns(eles[v], lat0.p0c, param, sub, beta, st, ie, it, 1, lib=lib)
+            out[:, idx] = sub
+        return out
+
+    return f
+
+
+def oracle_da_survival(lattices, ref, n_angle, angle_min, angle_max, n_radius, r_max, yscale, n_turns,
+                       variant: str = "cr", threads: int = 0):
+    """survive_turns[v, d, a, r] of a polar-grid scan through the oracle."""
+    from bgt import da
+    from oracle import oracle as O
+
+    lib = O.load(variant=variant)
+    lat0 = lattices[0]
+    param = O.make_param(lat0.species.mass, lat0.species.charge)
+    nv, nd = ref.shape[:2]
+    out = np.zeros((nv, nd, n_angle, n_radius), np.int32)
+    for v in range(nv):
+        v6 = da.grid_initial_conditions(ref[v:v + 1], n_angle, angle_min, angle_max, n_radius, r_max, yscale)
+        v6 = np.ascontiguousarray(v6)
+        n = v6.shape[1]
+        beta = O.beta_of(lat0.p0c, v6[5], lat0.species.mass)
+        st = np.ones(n, np.int32)
+        ie = np.full(n, -1, np.int32)
+        it = np.full(n, -1, np.int32)
+        O.track_turns(O.to_eles(lattices[v], lib), lat0.p0c, param, v6, beta, st, ie, it, n_turns,
+                      n_threads=threads, lib=lib)
+        surv = np.where(st == 1, n_turns, it)
+        out[v] = surv.reshape(nd, n_angle, n_radius)
+    return out

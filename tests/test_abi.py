@@ -1,4 +1,4 @@
-"""The C-ABI library loads and exports every symbol include/bgt.h declares
+"""The C-ABI library loads and exports every symbol include/*.h declares
 (no compute calls: runs without a GPU)."""
 import ctypes
 import re
@@ -10,7 +10,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def declared_symbols():
-    src = (ROOT / "include" / "bgt.h").read_text()
+    src = "\n".join(p.read_text() for p in sorted((ROOT / "include").glob("*.h")))
     return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(bgt_\w+)\s*\(", src, re.M)))
 
 

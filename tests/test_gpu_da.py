@@ -1,0 +1,92 @@
+"""Dynamic-aperture pieces on the GPU against the correctly rounded oracle:
+device tracking with per-particle variants, per-variant optics through the
+GPU one-turn map, and the one-launch polar-grid scan of error variants
+(bgt.da), all bit-identical."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from helpers import oracle_batch_one_turn, oracle_da_survival  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def variants():
+    from bgt import rings
+
+    return rings.error_variants(3, seed=21)
+
+
+def test_device_variants_equal_host_variants(variants):
+    from bgt import lattice as L
+    from bgt import rings
+    from bgt.track import Tracker
+
+    tr = Tracker(variants)
+    n = 3000
+    v0 = rings.gaussian_beam(rings.CONFIG1_BEAM, n=n)
+    var = np.sort(np.random.default_rng(1).integers(0, 3, n)).astype(np.int32)
+    hb = tr.make_bunch(v0.copy())
+    tr.track_turns(hb, 7, variant=var)
+    dev = torch.device("cuda", 0)
+    vec = torch.tensor(v0, device=dev).contiguous()
+    beta = torch.tensor(L.beta_of(tr.p0c, v0[5], tr.species.mass), device=dev)
+    st = torch.ones(n, dtype=torch.int32, device=dev)
+    ie = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    it = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    tr.track_turns_device(vec, beta, st, ie, it, 7, variant=torch.tensor(var, device=dev))
+    torch.cuda.synchronize()
+    assert np.array_equal(vec.cpu().numpy(), hb.vec6)
+    assert np.array_equal(st.cpu().numpy(), hb.state)
+    assert np.array_equal(it.cpu().numpy(), hb.ix_turn_lost)
+
+
+def test_device_variants_must_be_sorted(variants):
+    from bgt import _lib
+    from bgt.track import Tracker
+
+    tr = Tracker(variants)
+    dev = torch.device("cuda", 0)
+    n = 256
+    vec = torch.zeros(6, n, dtype=torch.float64, device=dev)
+    beta = torch.full((n,), 0.999, dtype=torch.float64, device=dev)
+    st = torch.ones(n, dtype=torch.int32, device=dev)
+    ie = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    it = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    var = torch.tensor(np.r_[np.ones(128), np.zeros(128)].astype(np.int32), device=dev)
+    with pytest.raises(_lib.BgtError, match="sorted"):
+        tr.track_turns_device(vec, beta, st, ie, it, 1, variant=var)
+
+
+def test_variant_optics_gpu_equals_oracle(variants):
+    from bgt import da
+    from bgt.track import Tracker
+
+    tr = Tracker(variants)
+    g = da.variant_optics(da.tracker_one_turn(tr), 3)
+    o = da.variant_optics(oracle_batch_one_turn(variants, variant="cr"), 3)
+    assert np.array_equal(g.closed_orbit, o.closed_orbit)
+    assert np.array_equal(g.eta, o.eta)
+    assert np.array_equal(g.beta_a, o.beta_a) and np.array_equal(g.tune_b, o.tune_b)
+
+
+def test_plain_scan_equals_oracle(variants):
+    from bgt import da
+    from bgt.track import Tracker
+
+    tr = Tracker(variants)
+    opt = da.variant_optics(da.tracker_one_turn(tr), 3)
+    ref = da.reference_orbits(opt, (-0.01, 0.0, 0.01))
+    ys = da.y_scale(opt.beta_a[0], opt.beta_b[0])
+    grid = dict(n_angle=5, angle_min=0.0, angle_max=math.pi, n_radius=12, r_max=0.03, yscale=ys)
+    res = da.plain_scan(tr, ref, n_turns=40, **grid)
+    surv = oracle_da_survival(variants, ref, n_turns=40, **grid)
+    assert np.array_equal(res.survive_turns, surv)
+    assert np.array_equal(res.radius, da.radius_from_survival(surv, 40, 0.03))
+    assert np.any(res.radius < 0.03) and np.any(res.radius > 0)
