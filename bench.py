@@ -53,6 +53,16 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
     ap.add_argument("--tuning", default="", help="threads_per_block,blocks_per_sm (skips the autotuner)")
+    ap.add_argument("--workload", default="track", choices=["track", "da", "learned-da", "sext-scan"],
+                    help="track: the headline tracking metric (default); da: batched DA scan of error variants; "
+                         "learned-da: classifier-pruned vs plain DA scan; sext-scan: pruned sextupole-setting scan")
+    ap.add_argument("--variants", type=int, default=0, help="DA workloads: number of lattice variants")
+    ap.add_argument("--da-turns", type=int, default=0, help="DA workloads: turns per probe (default 20000)")
+    ap.add_argument("--jitter", action="store_true", help="learned-da: add one jittered probe per grid cell")
+    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--model", default="", help="sext-scan: start from this saved classifier (fine-tune)")
+    ap.add_argument("--save-model", default="", help="learned-da / sext-scan: save the trained classifier")
     return ap.parse_args()
 
 
@@ -177,8 +187,195 @@ def cpu_baseline():
             "kind": "port", "sample": f"{n} particles x {turns} turns, element-outer OpenMP (reference loop order)"}
 
 
+# ---------------------------------------------------------------------------
+# Dynamic-aperture workloads (one GPU): the batched scan of error variants,
+# the classifier-pruned scan against the plain one, and the pruned
+# sextupole-setting scan.  Each prints one JSON line.
+
+def _da_problem(lats, grid, turns):
+    import dataclasses
+
+    from bgt import da, rings
+    from bgt import learned_da as LD
+    from bgt.track import Tracker
+
+    g = dataclasses.replace(grid, n_turns=turns)
+    ys = da.y_scale(rings.TWISS0["beta_a"], rings.TWISS0["beta_b"])
+    return LD.setup(Tracker(lats), lats, g, (rings.K2_SF, rings.K2_SD), yscale=ys)
+
+
+def _autotune_da(pb, turns=2):
+    from bgt import autotune
+    from bgt import da
+
+    v6 = da.grid_initial_conditions(pb.ref, pb.n_angle, pb.angle_min, pb.angle_max, pb.n_radius, pb.r_max,
+                                    pb.yscale)
+    var = np.repeat(np.arange(pb.n_variants, dtype=np.int32), pb.per_variant)
+    autotune.tune(pb.tracker, v6, turns=turns, sample=min(v6.shape[1], 262_144), variant=var,
+                  compact_options=(0, 16))
+    return pb.tracker.get_tuning()
+
+
+def _mm(x):
+    return float(np.mean(x)) * 1e3
+
+
+def run_da(args):
+    """Batched DA scan: every probe of every error variant in one launch."""
+    import torch
+
+    from bgt import da, rings
+
+    nv = args.variants or 256
+    turns = args.da_turns or rings.CONFIG2_GRID.n_turns
+    t0 = time.perf_counter()
+    lats = rings.error_variants(nv)
+    pb = _da_problem(lats, rings.CONFIG2_GRID, turns)
+    t_setup = time.perf_counter() - t0
+    tun = _autotune_da(pb)
+    launches0 = pb.tracker.launch_count
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        res = da.plain_scan(pb.tracker, pb.ref, **pb.grid())
+    n = nv * pb.per_variant
+    line = {"metric": "DA scan wall time, error variants x polar grid (one launch)", "value": res.wall_s,
+            "unit": "s", "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched DA scan of error variants", "variants": nv, "probes": n,
+                       "probes_per_variant": pb.per_variant, "turns": turns, "angles": pb.n_angle,
+                       "radii": pb.n_radius, "r_max_m": pb.r_max, "deltas": list(pb.deltas)},
+            "particle_turns": res.particle_turns, "particle_turns_per_s": res.particle_turns / res.wall_s,
+            "da_radius_mm_mean": _mm(res.radius),
+            "da_radius_mm_mean_per_delta": [_mm(res.radius[:, d]) for d in range(len(pb.deltas))],
+            "setup_s": t_setup, "tuning": tun, "gpu_launches": pb.tracker.launch_count - launches0,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def _train_classifier(args, pb, scans, net, fine_tune=False):
+    from bgt import learned_da as LD
+
+    raw, lab = LD.training_set(pb, scans, net)
+    hist, t_train = LD.train(net, raw, lab, epochs=args.epochs if not fine_tune else max(2, args.epochs // 2),
+                             batch=8192, lr=2e-3 if not fine_tune else 1e-3, seed=args.seed,
+                             set_normalization=not fine_tune)
+    n = (raw.shape[0] // 128) * 128
+    b = min(8192, n)
+    steps = len(hist) * (n // b)
+    flops = 852_000.0 * b * steps  # GEMM flops per sample (forward + backward) x samples
+    return {"samples": int(raw.shape[0]), "lost_fraction": float(lab.float().mean().item()), "epochs": len(hist),
+            "loss_per_epoch": hist, "wall_s": t_train, "samples_per_s": b * steps / t_train,
+            "gemm_tflops": flops / t_train / 1e12}
+
+
+def run_learned_da(args):
+    """Classifier-pruned DA scan vs the plain scan on held-out variants."""
+    import torch
+
+    from bgt import da, rings
+    from bgt import learned_da as LD
+    from bgt.mlp import SurvivalMLP
+
+    nv = args.variants or 256
+    turns = args.da_turns or rings.CONFIG2_GRID.n_turns
+    half = nv // 2
+    lats = rings.error_variants(nv)
+    pb_tr = _da_problem(lats[:half], rings.CONFIG2_GRID, turns)
+    pb_te = _da_problem(lats[half:], rings.CONFIG2_GRID, turns)
+    tun = _autotune_da(pb_te)
+    pb_tr.tracker.set_tuning(**tun)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        scans = [LD.staged_scan(pb_tr, 0, half)]
+        if args.jitter:
+            scans.append(LD.staged_scan(pb_tr, 0, half, jitter_seed=args.seed))
+        net = SurvivalMLP(max_batch=16384, seed=args.seed)
+        train = _train_classifier(args, pb_tr, scans, net)
+        plain = da.plain_scan(pb_te.tracker, pb_te.ref, **pb_te.grid())
+        pr = LD.pruned_scan(pb_te, net, 0, nv - half, seed=args.seed)
+    if args.save_model:
+        net.save(args.save_model)
+    plain_surv = (plain.survive_turns >= turns).reshape(-1)
+    agree = bool(np.array_equal(pr.survive_label[pr.tracked], plain_surv[pr.tracked]))
+    cells = np.abs(pr.radius - plain.radius) / (pb_te.r_max / (pb_te.n_radius - 1))
+    line = {"metric": "DA-scan wall time, plain / classifier-pruned, held-out variants",
+            "value": plain.wall_s / pr.wall_s, "unit": "x", "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f64 tracking, bf16/fp32 classifier", "data": "synthetic",
+            "config": {"workload": "learned DA scan of error variants", "variants_train": half,
+                       "variants_heldout": nv - half, "probes_per_variant": pb_te.per_variant, "turns": turns,
+                       "early_turns": 64, "p_hi": 0.98, "p_lo": 0.02, "audit": 0.02, "boundary_cells": 2,
+                       "jitter": bool(args.jitter)},
+            "plain_s": plain.wall_s, "pruned_s": pr.wall_s, "da_error": da.da_error(pr.radius, plain.radius),
+            "rays_exact_fraction": float(np.mean(cells < 0.5)), "max_error_cells": float(np.max(cells)),
+            "plain_particle_turns": plain.particle_turns, "pruned_particle_turns": pr.particle_turns,
+            "tracked_fraction": pr.n_tracked / pr.n_probes, "retired_lost": pr.n_retired_lost,
+            "retired_survive": pr.n_retired_survive, "audit_probes": pr.audit_n, "audit_errors": pr.audit_errors,
+            "tracked_outcomes_equal_plain": agree, "train_scan_s": sum(s.wall_s for s in scans), "train": train,
+            "da_radius_mm_mean": {"plain": _mm(plain.radius), "pruned": _mm(pr.radius)}, "tuning": tun,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_sext_scan(args):
+    """Sextupole-setting scan: fine-tune on the first 256 variants' tracking,
+    prune the rest with the boundary verified by the tracker, rank all
+    variants by DA, and compare the ranking of 256 audited variants with a
+    plain-tracking ranking of the same variants."""
+    import torch
+
+    from bgt import da, rings
+    from bgt import learned_da as LD
+    from bgt.mlp import SurvivalMLP
+
+    nv = args.variants or 4096
+    turns = args.da_turns or rings.CONFIG4_GRID.n_turns
+    first = min(256, nv // 4)
+    t0 = time.perf_counter()
+    lats = rings.sextupole_variants(nv)
+    pb_ft = _da_problem(lats[:first], rings.CONFIG4_GRID, turns)
+    pb_rest = _da_problem(lats[first:], rings.CONFIG4_GRID, turns)
+    rng = np.random.default_rng(args.seed)
+    n_audit = min(256, nv - first)
+    audit_idx = np.sort(rng.choice(nv - first, n_audit, replace=False))
+    pb_aud = _da_problem([lats[first + i] for i in audit_idx], rings.CONFIG4_GRID, turns)
+    t_setup = time.perf_counter() - t0
+    tun = _autotune_da(pb_rest)
+    pb_ft.tracker.set_tuning(**tun)
+    pb_aud.tracker.set_tuning(**tun)
+    net = SurvivalMLP(max_batch=16384, seed=args.seed)
+    fine = bool(args.model)
+    if fine:
+        net.load(args.model)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ft = LD.staged_scan(pb_ft, 0, first)
+        train = _train_classifier(args, pb_ft, [ft], net, fine_tune=fine)
+        pr = LD.pruned_scan(pb_rest, net, 0, nv - first, seed=args.seed)
+        plain = da.plain_scan(pb_aud.tracker, pb_aud.ref, **pb_aud.grid())
+    if args.save_model:
+        net.save(args.save_model)
+    ft_surv = (ft.survive >= turns).cpu().numpy()
+    da_ft = LD.radius_of(pb_ft, ft_surv, first).mean(axis=(1, 2))
+    da_rest = pr.radius.mean(axis=(1, 2))
+    da_all = np.concatenate([da_ft, da_rest])
+    order = np.argsort(-da_all, kind="stable")
+    ranking = LD.ranking_mismatches(da_rest[audit_idx], plain.radius.mean(axis=(1, 2)))
+    line = {"metric": "sextupole scan: ranking mismatches of pruned vs plain DA, audited variants",
+            "value": ranking["discordant_pairs"], "unit": "discordant pairs", "higher_is_better": False,
+            "n_gpus": 1, "dtype": "f64 tracking, bf16/fp32 classifier", "data": "synthetic",
+            "config": {"workload": "pruned sextupole-setting scan", "variants": nv, "fine_tune_variants": first,
+                       "probes_per_variant": pb_rest.per_variant, "turns": turns, "audited_variants": n_audit,
+                       "boundary_cells": 2, "start_model": args.model or None},
+            "ranking": ranking, "da_error_audited": da.da_error(pr.radius[audit_idx], plain.radius),
+            "pruned_s": pr.wall_s, "fine_tune_scan_s": ft.wall_s, "audit_plain_s": plain.wall_s,
+            "audit_plain_s_per_variant": plain.wall_s / n_audit, "pruned_s_per_variant": pr.wall_s / (nv - first),
+            "tracked_fraction": pr.n_tracked / pr.n_probes, "train": train,
+            "top10_variants_by_da": [[int(i), _mm(da_all[i])] for i in order[:10]],
+            "setup_s": t_setup, "tuning": tun, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload != "track":
+        {"da": run_da, "learned-da": run_learned_da, "sext-scan": run_sext_scan}[args.workload](args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -40,7 +40,7 @@ class BgtSpecies(C.Structure):
 
 class BgtTuning(C.Structure):
     _fields_ = [("threads_per_block", C.c_int32), ("blocks_per_sm", C.c_int32), ("turns_per_launch", C.c_int32),
-                ("compact_every", C.c_int32)]
+                ("compact_every", C.c_int32), ("table_mode", C.c_int32)]
 
 
 class BgtError(RuntimeError):
@@ -132,6 +132,17 @@ def to_bgt_element(e: L.Element) -> BgtElement:
         b.an_elec[:] = list(ae)
         b.bn_elec[:] = list(be)
     return b
+
+
+def element_key(e: L.Element) -> tuple:
+    """Everything to_bgt_element reads from an element: equal keys give equal
+    C structs (used to convert each distinct element of a variant family
+    once)."""
+    return (e.key, e.ix_ele, e.is_on, e.num_steps, e.fringe_type, e.fringe_at, e.aperture_type, e.aperture_at,
+            e.offset_moves_aperture, e.exact_multipoles, e.scale_multipoles, e.has_misalign,
+            tuple(sorted(e.values.items())), tuple(sorted(e.a_pole.items())), tuple(sorted(e.b_pole.items())),
+            tuple(sorted(e.ksl_pole.items())), tuple(sorted(e.a_pole_elec.items())),
+            tuple(sorted(e.b_pole_elec.items())))
 
 
 def ptr(a: np.ndarray, t):

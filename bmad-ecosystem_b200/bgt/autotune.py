@@ -2,7 +2,9 @@
 
 Candidates are the (particles per CTA, resident CTAs per SM) pairs the library
 is compiled for -- i.e. register caps of 128/96/80/64 per thread traded
-against occupancy -- and, for lossy workloads, the compaction interval.  Each
+against occupancy --, for some of them the element table read from global
+memory instead of shared memory (frees shared memory for more resident CTAs
+when tables are large), and, for lossy workloads, the compaction interval.  Each
 candidate tracks a sample of the real bunch for a few turns on the device
 (CUDA events on the launching stream); the fastest per particle.turn wins.
 Results are cached per (table bytes, lattice name, particle count) in memory
@@ -17,8 +19,13 @@ from typing import Dict, Iterable, Optional, Tuple
 
 import numpy as np
 
+from . import _lib
+
 SHAPES: Tuple[Tuple[int, int], ...] = ((64, 8), (64, 10), (64, 12), (64, 16), (128, 4), (128, 5), (128, 6),
                                        (128, 8), (256, 2), (256, 3), (256, 4))
+
+# shapes compiled with the element table read from global memory (table_mode 2)
+GLOBAL_TABLE_SHAPES: Tuple[Tuple[int, int], ...] = ((128, 4), (128, 5), (256, 2), (256, 3))
 
 _cache: Dict[str, dict] = {}
 
@@ -27,11 +34,33 @@ def _key(tracker, n: int, lossy: bool) -> str:
     return f"{tracker.lattice.name}:{tracker.table_bytes()}:{tracker.n_variants}:{n}:{int(lossy)}"
 
 
+def _time_shape(tracker, base, beta0, var_t, m, turns, stream, dev) -> float:
+    import torch
+
+    best = None
+    for rep in range(2):  # first repetition warms up
+        v = base.clone()
+        b = beta0.clone()
+        st = torch.ones(m, dtype=torch.int32, device=dev)
+        ie = torch.full((m,), -1, dtype=torch.int32, device=dev)
+        it = torch.full((m,), -1, dtype=torch.int32, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tracker.track_turns_device(v, b, st, ie, it, turns, stream=stream, variant=var_t)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best
+
+
 def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, int]] = SHAPES,
          compact_options: Iterable[int] = (0,), sample: int = 200_000, cache_file: Optional[str] = None,
-         verbose: bool = False) -> dict:
+         verbose: bool = False, variant: Optional[np.ndarray] = None) -> dict:
     """Pick the fastest tuning for tracking `vec6` (6, n) with `tracker`;
-    sets it on the tracker and returns it."""
+    sets it on the tracker and returns it.  `variant` (sorted int32 [n])
+    assigns the particles to lattice variants; the sample is then spread
+    evenly over the bunch so that every variant's share is represented."""
     import torch
 
     n = vec6.shape[1]
@@ -48,33 +77,29 @@ def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, 
 
     m = min(n, sample)
     dev = torch.device("cuda", tracker.device)
-    base = torch.tensor(np.ascontiguousarray(vec6[:, :m]), dtype=torch.float64, device=dev)
+    pick = np.linspace(0, n - 1, m).astype(np.int64) if variant is not None else np.arange(m)
+    base = torch.tensor(np.ascontiguousarray(vec6[:, pick]), dtype=torch.float64, device=dev)
+    var_t = (torch.tensor(np.ascontiguousarray(variant[pick], dtype=np.int32), device=dev)
+             if variant is not None else None)
     pz = base[5]
     pc = (1 + pz) * tracker.p0c
     beta0 = pc / torch.sqrt(pc * pc + tracker.species.mass ** 2)
     stream = torch.cuda.current_stream(dev)
     results = []
-    for (tpb, bps) in shapes:
-        for ce in compact_options:
-            tun = dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0)
-            tracker.set_tuning(**tun)
-            best = None
-            for rep in range(2):  # first repetition warms up
-                v = base.clone()
-                b = beta0.clone()
-                st = torch.ones(m, dtype=torch.int32, device=dev)
-                ie = torch.full((m,), -1, dtype=torch.int32, device=dev)
-                it = torch.full((m,), -1, dtype=torch.int32, device=dev)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                tracker.track_turns_device(v, b, st, ie, it, turns, stream=stream)
-                e1.record(stream)
-                e1.synchronize()
-                ms = e0.elapsed_time(e1)
-                best = ms if best is None else min(best, ms)
-            results.append((best, tun))
-            if verbose:
-                print(f"  tune {tun}: {best:.3f} ms")
+    cands = [(tpb, bps, ce, tm) for (tpb, bps) in shapes for ce in compact_options
+             for tm in ((0, 2) if (tpb, bps) in GLOBAL_TABLE_SHAPES else (0,))]
+    for (tpb, bps, ce, tm) in cands:
+        tun = dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0, table_mode=tm)
+        tracker.set_tuning(**tun)
+        try:
+            best = _time_shape(tracker, base, beta0, var_t, m, turns, stream, dev)
+        except _lib.BgtError:
+            continue  # shape not available for this table (e.g. table larger than shared memory)
+        results.append((best, tun))
+        if verbose:
+            print(f"  tune {tun}: {best:.3f} ms")
+    if not results:
+        raise _lib.BgtError("no launch shape can run this table")
     results.sort(key=lambda r: r[0])
     choice = results[0][1]
     tracker.set_tuning(**choice)

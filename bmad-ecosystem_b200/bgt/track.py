@@ -82,9 +82,14 @@ class Tracker:
         self.n_ele = n_ele
         self.n_variants = len(lats)
         arr = (_lib.BgtElement * (n_ele * len(lats)))()
+        seen = {}
         for v, lat in enumerate(lats):
             for i, e in enumerate(lat.elements):
-                arr[v * n_ele + i] = _lib.to_bgt_element(e)
+                k = _lib.element_key(e)
+                c = seen.get(k)
+                if c is None:
+                    c = seen[k] = _lib.to_bgt_element(e)
+                arr[v * n_ele + i] = c
         sp = _lib.BgtSpecies(lats[0].species.mass, lats[0].species.charge, 1, 1e3)
         self.species = lats[0].species
         self.p0c = lats[0].p0c
@@ -98,8 +103,8 @@ class Tracker:
             self.set_tuning(**tuning)
 
     # -- tuning -----------------------------------------------------------
-    def set_tuning(self, threads_per_block=0, blocks_per_sm=0, turns_per_launch=0, compact_every=0):
-        t = _lib.BgtTuning(threads_per_block, blocks_per_sm, turns_per_launch, compact_every)
+    def set_tuning(self, threads_per_block=0, blocks_per_sm=0, turns_per_launch=0, compact_every=0, table_mode=0):
+        t = _lib.BgtTuning(threads_per_block, blocks_per_sm, turns_per_launch, compact_every, table_mode)
         _check(self.lib, self.h, self.lib.bgt_set_tuning(self.h, C.byref(t)), "bgt_set_tuning")
 
     def get_tuning(self) -> dict:

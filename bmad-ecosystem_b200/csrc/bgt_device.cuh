@@ -318,10 +318,56 @@ __device__ __forceinline__ void offset_unset(Part& p, const double* mis, int32_t
 // magnetic) and :314-401 (ab_multipole_kick).  The factor
 // r = ele%value(p0c)/orbit%p0c and the charge/orientation factor are exactly
 // 1.0 here, so a2 = scale * a, b2 = scale * b.
+// x^k for k = 0..7 exactly as mexp / gfortran's integer power (binary
+// exponentiation, y = y * x order) evaluates each one: x^3 = x * x^2,
+// x^5 = x * x^4, x^6 = x^2 * x^4, x^7 = (x * x^2) * x^4.
+__device__ __forceinline__ void powi_table7(double x, double (&p)[8]) {
+  p[0] = 1.0;
+  p[1] = x;
+  p[2] = x * x;
+  p[3] = x * p[2];
+  p[4] = p[2] * p[2];
+  p[5] = x * p[4];
+  p[6] = p[2] * p[4];
+  p[7] = p[3] * p[4];
+}
+
 __device__ __forceinline__ void ab_multipole_kicks(Part& p, const double* an, const double* bn, int ix_max,
                                                    double scale) {
   double kx_tot = 0, ky_tot = 0;
   const double x = p.x, y = p.y;
+  if (ix_max <= 7) {
+    // same terms in the same order, each power computed once per kick
+    double xp[8], yp[8];
+    powi_table7(x, xp);
+    powi_table7(y, yp);
+#pragma unroll
+    for (int n = 0; n <= 7; n++) {
+      if (n > ix_max) break;
+      const double a = an[n], b = bn[n];
+      double kx = 0, ky = 0;
+      if (!(a == 0 && b == 0)) {
+        const double a2 = scale * a, b2 = scale * b;
+#pragma unroll
+        for (int m = 0; m <= n; m += 2) {
+          const double f = c_cm[n][m] * xp[n - m] * yp[m];
+          kx = kx + b2 * f;
+          ky = ky - a2 * f;
+        }
+#pragma unroll
+        for (int m = 1; m <= n; m += 2) {
+          const double f = c_cm[n][m] * xp[n - m] * yp[m];
+          kx = kx + a2 * f;
+          ky = ky + b2 * f;
+        }
+      }
+      kx_tot = kx_tot + kx;
+      ky_tot = ky_tot + ky;
+    }
+    p.px = p.px + kx_tot;
+    p.py = p.py + ky_tot;
+    return;
+  }
   for (int n = 0; n <= ix_max; n++) {
     double a = an[n], b = bn[n];
     double kx = 0, ky = 0;

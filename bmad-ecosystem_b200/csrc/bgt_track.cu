@@ -557,15 +557,20 @@ struct KArgs {
 
 constexpr int MAX_BLOCK = 256;
 
-template <int BLOCK, int MINB>
+// GTAB: the variant's element table is read from global memory (L2 / L1)
+// instead of being staged in shared memory -- for tables larger than the
+// shared-memory budget (e.g. every quadrupole and sextupole misaligned and
+// carrying its own multipole errors), or to leave shared memory to more
+// resident CTAs.
+template <int BLOCK, int MINB, bool GTAB>
 __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
   extern __shared__ __align__(128) double smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t s_tile;
   __shared__ int32_t s_warp_cnt[BLOCK / 32];
-  double* table = smem;
+  const double* table = smem;
   // compaction staging area sits after the table
-  double* stage = smem + a.table_dw;  // [9][BLOCK] doubles; rows 7-8 hold int32 ids and loss records
+  double* stage = smem + (GTAB ? 0 : a.table_dw);  // [9][BLOCK] doubles; rows 7-8 hold int32 ids and loss records
   int32_t* stage_i = reinterpret_cast<int32_t*>(stage + 7 * BLOCK);  // [3][BLOCK]
   // quad memo after the (optional) compaction stage
   double* qmemo_base = stage + (a.compact_every > 0 ? 9 * BLOCK : 0);
@@ -585,11 +590,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
     const int64_t tile = s_tile;
     if (tile >= n_tiles) break;
     const int variant = a.tile_variant ? a.tile_variant[tile] : 0;
-    if (variant != loaded_variant) {
+    if (GTAB) {
+      table = a.tables + a.table_off_dw[variant];
+    } else if (variant != loaded_variant) {
       // all threads finished reading the previous table (barrier above)
       if (tid == 0) {
         mbar_expect_tx(&bar, table_bytes);
-        tma_bulk_g2s(table, a.tables + a.table_off_dw[variant], table_bytes, &bar);
+        tma_bulk_g2s(smem, a.tables + a.table_off_dw[variant], table_bytes, &bar);
       }
       const int bad = __syncthreads_or(!mbar_wait(&bar, parity, 1u << 26));
       if (bad) {
@@ -1251,7 +1258,7 @@ struct bgt_handle {
   double* d_tables = nullptr;
   int64_t* d_table_off = nullptr;
   int32_t* d_scratch = nullptr;  // [0] tile counter, [1] error flag
-  bgt_tuning tuning{128, 4, 0, 0};
+  bgt_tuning tuning{128, 4, 0, 0, 0};
   std::string err;
   int64_t launches = 0;
   // host-API staging
@@ -1278,23 +1285,29 @@ static int set_err(bgt_handle* h, int code, const std::string& msg) {
       return set_err((h), BGT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
   } while (0)
 
-static size_t smem_bytes(const bgt_handle* h, int block, bool compact) {
-  size_t b = (size_t)h->table_dw * 8;
+// dynamic shared memory per CTA: B200 allows 227 KB per block, less the
+// kernel's static shared memory
+constexpr size_t SMEM_LIMIT = 224 * 1024;
+
+static size_t smem_bytes(const bgt_handle* h, int block, bool compact, bool gtab = false) {
+  size_t b = gtab ? 0 : (size_t)h->table_dw * 8;
   if (compact) b += (size_t)9 * block * 8;
   b += (size_t)QMEMO_CLASSES * 13 * block * 8;
   return b;
 }
 
-template <int BLOCK, int MINB>
+template <int BLOCK, int MINB, bool GTAB = false>
 static cudaError_t launch_track(const KArgs& a, int grid, size_t smem, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         200 * 1024);
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK, MINB, GTAB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_set[dev & 63] = true;
   }
-  track_kernel<BLOCK, MINB><<<grid, BLOCK, smem, st>>>(a);
+  track_kernel<BLOCK, MINB, GTAB><<<grid, BLOCK, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1302,8 +1315,12 @@ static cudaError_t launch_track(const KArgs& a, int grid, size_t smem, cudaStrea
 static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t st) {
   int block = h->tuning.threads_per_block;
   bool compact = a.compact_every > 0;
-  size_t smem = smem_bytes(h, block, compact);
-  if (smem > 200 * 1024) return set_err(h, BGT_ETOOLARGE, "element table does not fit in shared memory");
+  const bool fits = smem_bytes(h, block, compact) <= SMEM_LIMIT;
+  if (h->tuning.table_mode == 1 && !fits)
+    return set_err(h, BGT_ETOOLARGE, "element table does not fit in shared memory (table_mode 1)");
+  const bool gtab = h->tuning.table_mode == 2 || !fits;
+  size_t smem = smem_bytes(h, block, compact, gtab);
+  if (smem > SMEM_LIMIT) return set_err(h, BGT_ETOOLARGE, "tracking state does not fit in shared memory");
   int64_t grid = (int64_t)h->num_sms * std::max(1, h->tuning.blocks_per_sm);
   if (grid > n_tiles) grid = n_tiles;
   if (grid < 1) grid = 1;
@@ -1314,6 +1331,21 @@ static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t s
   // (threads per CTA, resident CTAs per SM) pairs compiled with matching
   // __launch_bounds__, i.e. register caps of 128, 102, 85 and 64 per thread
   const int bps = h->tuning.blocks_per_sm;
+  if (gtab) {
+    switch (block * 100 + bps) {
+      case 12804: e = launch_track<128, 4, true>(a, (int)grid, smem, st); break;
+      case 12805: e = launch_track<128, 5, true>(a, (int)grid, smem, st); break;
+      case 25602: e = launch_track<256, 2, true>(a, (int)grid, smem, st); break;
+      case 25603: e = launch_track<256, 3, true>(a, (int)grid, smem, st); break;
+      default:
+        return set_err(h, BGT_ETOOLARGE,
+                       "element table read from global memory: tuning must be (128: 4,5) or (256: 2,3)");
+    }
+    if (e != cudaSuccess)
+      return set_err(h, BGT_ECUDA, std::string("track_kernel launch: ") + cudaGetErrorString(e));
+    h->launches++;
+    return 0;
+  }
   switch (block * 100 + bps) {
     case 6408: e = launch_track<64, 8>(a, (int)grid, smem, st); break;
     case 6410: e = launch_track<64, 10>(a, (int)grid, smem, st); break;
@@ -1482,6 +1514,7 @@ int bgt_set_tuning(bgt_handle* h, const bgt_tuning* t) {
   if (n.threads_per_block != 64 && n.threads_per_block != 128 && n.threads_per_block != 256)
     return set_err(h, BGT_EINVAL, "threads_per_block must be 64, 128 or 256");
   if (n.compact_every < 0 || n.turns_per_launch < 0) return set_err(h, BGT_EINVAL, "negative tuning value");
+  if (n.table_mode < 0 || n.table_mode > 2) return set_err(h, BGT_EINVAL, "table_mode must be 0, 1 or 2");
   h->tuning = n;
   return 0;
 }

@@ -144,6 +144,8 @@ typedef struct bgt_tuning {
   int32_t blocks_per_sm;     /* resident CTAs per SM for the persistent grid */
   int32_t turns_per_launch;  /* turns per persistent-kernel launch (graph node) */
   int32_t compact_every;     /* compact lost particles every this many turns (0 = never) */
+  int32_t table_mode;        /* element table: 0 = staged in shared memory when it fits, else read
+                                from global memory; 1 = shared memory only; 2 = global memory */
 } bgt_tuning;
 
 typedef struct bgt_handle bgt_handle;
@@ -232,7 +234,8 @@ int64_t bgt_kernel_launch_count(const bgt_handle* h);
  * threads) race: serialise them.  The first call on a device looks up the
  * array's address and uploads constant tables; make it before any stream
  * capture.  tuning may be NULL; otherwise (threads, CTAs per SM) must be
- * (128, 4) or (256, 2).  On error a message is written to err (err_len bytes).
+ * (128, 4) or (256, 2) (table_mode is ignored: the table is always staged in
+ * shared memory).  On error a message is written to err (err_len bytes).
  */
 int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n_ele, const bgt_species* species,
                                    double* d_vec6, double* d_beta, int32_t* d_state, int32_t* d_ix_ele_lost,

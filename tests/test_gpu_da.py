@@ -90,3 +90,59 @@ def test_plain_scan_equals_oracle(variants):
     assert np.array_equal(res.survive_turns, surv)
     assert np.array_equal(res.radius, da.radius_from_survival(surv, 40, 0.03))
     assert np.any(res.radius < 0.03) and np.any(res.radius > 0)
+
+
+def _two_error_rings():
+    """Two error variants' element lists in one ring: ~1540 elements, ~300 KB
+    of distinct element records -- more than one CTA's shared memory."""
+    import copy
+
+    from bgt import lattice as L
+    from bgt import rings
+
+    a, b = rings.error_variants(2, seed=33)
+    els = [copy.deepcopy(e) for e in a.elements[:-2]] + [copy.deepcopy(e) for e in b.elements]
+    return L.Lattice(els, a.species, a.p0c, a.e_tot, "two_error_rings").finalize()
+
+
+@pytest.mark.parametrize("mode", ["auto", "global"])
+def test_large_table_global_memory_path(mode):
+    """Element tables too large for shared memory are read from global memory
+    (table_mode 0 picks it, 2 forces it); results stay bit-identical to the
+    correctly rounded oracle, and table_mode 1 refuses such a table."""
+    from bgt import _lib, rings
+    from bgt.track import Tracker
+    from helpers import oracle_track_elements
+
+    lat = _two_error_rings()
+    tr = Tracker(lat)
+    assert tr.table_bytes() > 224 * 1024
+    tr.set_tuning(threads_per_block=256, blocks_per_sm=2, table_mode=2 if mode == "global" else 0)
+    v0 = rings.gaussian_beam(rings.CONFIG1_BEAM, n=1024)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 3)
+    ov, _, ost, oie, _ = oracle_track_elements(lat, v0.copy(), 0, len(lat), n_turns=3, variant="cr")
+    assert np.array_equal(b.vec6, ov) and np.array_equal(b.state, ost) and np.array_equal(b.ix_ele_lost, oie)
+    tr.set_tuning(threads_per_block=256, blocks_per_sm=2, table_mode=1)
+    with pytest.raises(_lib.BgtError, match="shared memory"):
+        tr.track_turns(tr.make_bunch(v0.copy()), 1)
+
+
+def test_error_variant_ring_matches_oracle():
+    """A full error-variant ring (every quadrupole with 16 kick-drift steps
+    and multipoles b3..b6 / a3..a6, offsets and rolls) over 20 turns:
+    bit-identical to the correctly rounded oracle, in both table modes."""
+    from bgt import rings
+    from bgt.track import Tracker
+    from helpers import oracle_track_elements
+
+    lat = rings.error_variants(1, seed=44)[0]
+    v0 = rings.gaussian_beam(rings.CONFIG1_BEAM, n=2048)
+    ov, _, ost, oie, oit = oracle_track_elements(lat, v0.copy(), 0, len(lat), n_turns=20, variant="cr")
+    tr = Tracker(lat)
+    for mode in (1, 2):
+        tr.set_tuning(threads_per_block=128, blocks_per_sm=4, table_mode=mode)
+        b = tr.make_bunch(v0.copy())
+        tr.track_turns(b, 20)
+        assert np.array_equal(b.vec6, ov) and np.array_equal(b.state, ost)
+        assert np.array_equal(b.ix_ele_lost, oie) and np.array_equal(b.ix_turn_lost, oit)
