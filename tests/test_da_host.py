@@ -88,3 +88,33 @@ def test_error_summary_scales():
     assert np.all(se[:, :14] > 0.3) and np.all(se[:, :14] < 3.0) and np.allclose(se[:, 14:], 0)
     ss = da.error_summary(sx, (rings.K2_SF, rings.K2_SD))
     assert np.allclose(ss[:, :14], 0) and np.all(np.abs(ss[:, 14:]) <= 1.0 + 1e-12)
+
+
+def test_ranking_mismatches():
+    from bgt import learned_da as LD
+
+    a = np.array([5.0, 4.0, 3.0, 2.0, 1.0])
+    r = LD.ranking_mismatches(a, a.copy())
+    assert r["discordant_pairs"] == 0 and r["spearman"] == pytest.approx(1.0) and r["pairs"] == 10
+    b = np.array([4.0, 5.0, 3.0, 1.0, 2.0])  # two adjacent swaps
+    r = LD.ranking_mismatches(a, b)
+    assert r["discordant_pairs"] == 2 and r["rank_position_mismatches"] == 4
+    r = LD.ranking_mismatches(a, a[::-1].copy())
+    assert r["discordant_pairs"] == 10 and r["spearman"] == pytest.approx(-1.0)
+
+
+def test_radius_of_survive_labels():
+    from bgt import learned_da as LD
+
+    class P:
+        deltas = (0.0, 0.01)
+        n_angle = 2
+        n_radius = 5
+        r_max = 0.004
+
+    lab = np.ones((1, 2, 2, 5), bool)
+    lab[0, 0, 1, 3] = False
+    lab[0, 1, 0, 0] = False
+    r = LD.radius_of(P, lab.reshape(-1), 1)
+    assert r.shape == (1, 2, 2)
+    assert r[0, 0, 0] == 0.004 and r[0, 0, 1] == 0.002 and r[0, 1, 0] == 0.0 and r[0, 1, 1] == 0.004
