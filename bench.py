@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
-    ap.add_argument("--tuning", default="", help="threads_per_block,blocks_per_sm (skips the autotuner)")
+    ap.add_argument("--tuning", default="", help="threads_per_block,blocks_per_sm (skips the autotuner); DA "
+                    "workloads also take ,table_mode[,compact_every]")
     ap.add_argument("--workload", default="track", choices=["track", "da", "learned-da", "sext-scan"],
                     help="track: the headline tracking metric (default); da: batched DA scan of error variants; "
                          "learned-da: classifier-pruned vs plain DA scan; sext-scan: pruned sextupole-setting scan")
@@ -206,9 +207,15 @@ def _da_problem(lats, grid, turns):
     return LD.setup(Tracker(lats), lats, g, (rings.K2_SF, rings.K2_SD), yscale=ys)
 
 
-def _autotune_da(pb, turns=2):
+def _autotune_da(pb, turns=2, fixed=""):
     from bgt import autotune
     from bgt import da
+
+    if fixed:
+        # threads_per_block,blocks_per_sm[,table_mode[,compact_every]]: no sweep
+        f = [int(x) for x in fixed.split(",")] + [0, 0]
+        pb.tracker.set_tuning(threads_per_block=f[0], blocks_per_sm=f[1], table_mode=f[2], compact_every=f[3])
+        return pb.tracker.get_tuning()
 
     v6 = da.grid_initial_conditions(pb.ref, pb.n_angle, pb.angle_min, pb.angle_max, pb.n_radius, pb.r_max,
                                     pb.yscale)
@@ -234,7 +241,7 @@ def run_da(args):
     lats = rings.error_variants(nv)
     pb = _da_problem(lats, rings.CONFIG2_GRID, turns)
     t_setup = time.perf_counter() - t0
-    tun = _autotune_da(pb)
+    tun = _autotune_da(pb, fixed=args.tuning)
     launches0 = pb.tracker.launch_count
     with ClockSampler(torch.cuda.current_device()) as clk:
         res = da.plain_scan(pb.tracker, pb.ref, **pb.grid())
@@ -282,7 +289,7 @@ def run_learned_da(args):
     lats = rings.error_variants(nv)
     pb_tr = _da_problem(lats[:half], rings.CONFIG2_GRID, turns)
     pb_te = _da_problem(lats[half:], rings.CONFIG2_GRID, turns)
-    tun = _autotune_da(pb_te)
+    tun = _autotune_da(pb_te, fixed=args.tuning)
     pb_tr.tracker.set_tuning(**tun)
     with ClockSampler(torch.cuda.current_device()) as clk:
         scans = [LD.staged_scan(pb_tr, 0, half)]
@@ -357,7 +364,7 @@ def run_sext_scan(args):
     audit_idx = np.sort(rng.choice(nv - first, n_audit, replace=False))
     pb_aud = _da_problem([lats[first + i] for i in audit_idx], rings.CONFIG4_GRID, turns)
     t_setup = time.perf_counter() - t0
-    tun = _autotune_da(pb_rest)
+    tun = _autotune_da(pb_rest, fixed=args.tuning)
     pb_ft.tracker.set_tuning(**tun)
     pb_aud.tracker.set_tuning(**tun)
     net = SurvivalMLP(max_batch=16384, seed=args.seed)
