@@ -229,6 +229,33 @@ def _mm(x):
     return float(np.mean(x)) * 1e3
 
 
+def da_cpu_baseline(lat, pb, n_probe=512, turns=20):
+    """The oracle in the reference's loop order (element-outer OpenMP) on all
+    host cores, tracking a sample of one error variant's DA probes (spread
+    over its grid) for a few turns: particle.turns/s of the plain scan on the
+    CPU."""
+    from bgt import da
+    from oracle import oracle as O
+
+    eles = O.to_eles(lat)
+    param = O.make_param(lat.species.mass, lat.species.charge)
+    threads = os.cpu_count() or 1
+    v6 = da.grid_initial_conditions(pb.ref[:1], pb.n_angle, pb.angle_min, pb.angle_max, pb.n_radius, pb.r_max,
+                                    pb.yscale)
+    pick = np.linspace(0, v6.shape[1] - 1, n_probe).astype(np.int64)
+    v = np.ascontiguousarray(v6[:, pick])
+    b = O.beta_of(lat.p0c, v[5], lat.species.mass)
+    st = np.ones(n_probe, np.int32)
+    ie = np.full(n_probe, -1, np.int32)
+    it = np.full(n_probe, -1, np.int32)
+    t = time.perf_counter()
+    O.track_turns(eles, lat.p0c, param, v, b, st, ie, it, turns, n_threads=threads, element_outer=True)
+    dt = time.perf_counter() - t
+    return {"value": turns_tracked(np.ones(n_probe, bool), it, st, 0, turns) / dt, "unit": "particle*turns/s",
+            "cores": threads, "kind": "port",
+            "sample": f"{n_probe} grid probes of variant 0 x {turns} turns, element-outer OpenMP"}
+
+
 def run_da(args):
     """Batched DA scan: every probe of every error variant in one launch."""
     import torch
@@ -256,6 +283,10 @@ def run_da(args):
             "da_radius_mm_mean_per_delta": [_mm(res.radius[:, d]) for d in range(len(pb.deltas))],
             "setup_s": t_setup, "tuning": tun, "gpu_launches": pb.tracker.launch_count - launches0,
             "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        cpu = da_cpu_baseline(lats[0], pb)
+        line["cpu_baseline"] = cpu
+        line["cpu_estimate_s"] = res.particle_turns / cpu["value"]
     print(json.dumps(line), flush=True)
 
 
@@ -338,6 +369,10 @@ def run_learned_da(args):
                                         plain.radius]))},
             "train_scan_s": sum(s.wall_s for s in scans), "train": train,
             "da_radius_mm_mean_plain": _mm(plain.radius), "tuning": tun, "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        cpu = da_cpu_baseline(lats[half], pb_te)
+        line["cpu_baseline"] = cpu
+        line["cpu_estimate_plain_s"] = plain.particle_turns / cpu["value"]
     print(json.dumps(line), flush=True)
 
 
