@@ -563,10 +563,10 @@ def main():
         units_per_launch = units / max(1, launches)
         launch_s = t_local / max(1, launches)
         achieved = FLOPS_PER_PARTICLE_TURN * units_per_launch / launch_s / 1e12
-        # DRAM bytes per launch: 68.5 B per particle (dram__bytes_read.sum of one
-        # ncu capture of this kernel on 400k particles, profiles/
-        # track_kernel_fodo64_400k.md; the written records stay in L2 at
-        # kernel end), scaled to this launch's particle count
+        # DRAM bytes per launch: 68.5 B per particle (dram__bytes_read.sum +
+        # dram__bytes_write.sum of one ncu capture of this kernel on 400k
+        # particles; the written records stay in L2 at kernel end), scaled to
+        # this launch's particle count
         roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": 68.52 * n,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 400k-particle launch "
