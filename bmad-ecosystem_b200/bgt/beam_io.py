@@ -1,0 +1,284 @@
+"""Beam files and checkpoints for the tracker's particle arrays.
+
+* Bmad's ASCII beam format, written as ``write_ascii_beam_file`` and read as
+  ``read_beam_ascii`` do (bmad/multiparticle/beam_file_io.f90:123-350 and
+  :834-1275): per bunch a header of ``# key = value`` lines, a ``#!`` column
+  line and one row per particle (``es23.15`` reals).  Columns that hold the
+  same value for every particle (charge, species, ix_branch, direction,
+  time_dir) move to the header, all-zero field / phase / dt_ref columns are
+  dropped, spin is always written (:185-195).  Particle states are written and
+  read with the reference's ``state_name`` table (bmad_struct.f90:535-536),
+  whose entries 7 and 8 read 'Lost_Pz' and 'Lost_Z' while the codes are
+  lost_z = 7 and lost_pz = 8: files written by Bmad round-trip through this
+  module unchanged.  ``es23.15`` keeps 16 significant digits, so an ASCII
+  round trip moves coordinates by up to ~5e-16 relative.
+* Checkpoints (``save_checkpoint`` / ``load_checkpoint``): the exact FP64 /
+  int32 arrays and the next turn index in one ``.npz`` file, so that tracking
+  resumed from a checkpoint (``turn0`` = the saved turn) is bit-identical to
+  an uninterrupted run -- the role of long_term_tracking's restart from a
+  saved beam (``ltt%ix_turn_start``, bsim/modules/lt_tracking_mod.f90).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from .track import Bunch
+
+# bmad_struct.f90:535-536 (zero based); note the order of entries 7 and 8
+STATE_NAME = ["Pre_Born", "Alive", "Lost", "Lost_Neg_X", "Lost_Pos_X", "Lost_Neg_Y", "Lost_Pos_Y", "Lost_Pz",
+              "Lost_Z"]
+# bmad_struct.f90:398-399
+LOCATION_NAME = ["GARBAGE!", "Upstream_End", "Downstream_End", "Inside"]
+# species names (physical_constants / particle_species_mod), the ones this tracker handles
+SPECIES_MASS = {"electron": 0.51099895069e6, "positron": 0.51099895069e6, "proton": 938.27208816e6,
+                "antiproton": 938.27208816e6}
+
+
+@dataclass
+class BeamBunch:
+    """One bunch of a beam file: coordinates and per-particle bookkeeping."""
+    vec6: np.ndarray  # (6, n)
+    state: np.ndarray  # int32 (n,)
+    p0c: np.ndarray  # (n,)
+    s: np.ndarray
+    t: np.ndarray
+    charge: np.ndarray
+    spin: np.ndarray  # (3, n)
+    ix_ele: np.ndarray  # int32
+    beta: Optional[np.ndarray] = None
+    species: str = "electron"
+    location: str = "Downstream_End"
+    ix_branch: int = 0
+    direction: int = 1
+    time_dir: int = 1
+    charge_tot: Optional[float] = None
+
+    @property
+    def n(self) -> int:
+        return self.vec6.shape[1]
+
+    @classmethod
+    def from_bunch(cls, b: Bunch, p0c: float, species: str = "electron", s: float = 0.0, t: float = 0.0,
+                   charge: float = 0.0) -> "BeamBunch":
+        n = b.n
+        return cls(np.array(b.vec6, dtype=np.float64), np.array(b.state, np.int32), np.full(n, p0c),
+                   np.full(n, s), np.full(n, t), np.full(n, charge), np.zeros((3, n)),
+                   np.array(b.ix_ele_lost, np.int32), np.array(b.beta), species)
+
+    def to_bunch(self) -> Bunch:
+        """Tracker arrays; beta from the file or, as the reader's
+        bunch_finalizer does, from (1 + pz) p0c and the species mass."""
+        beta = self.beta
+        if beta is None:
+            pc = (1 + self.vec6[5]) * self.p0c
+            m = SPECIES_MASS[self.species.lower()]
+            beta = pc / np.sqrt(pc * pc + m * m)
+        n = self.n
+        ixe = np.where(self.state == 1, -1, self.ix_ele).astype(np.int32)
+        return Bunch(np.ascontiguousarray(self.vec6, dtype=np.float64), np.ascontiguousarray(beta, np.float64),
+                     np.ascontiguousarray(self.state, np.int32), ixe, np.full(n, -1, np.int32))
+
+
+def _key(who: str) -> str:
+    return ("# " + who).ljust(17)
+
+
+def _es(v: float) -> str:
+    """Fortran es23.15."""
+    return f"{v:23.15E}"
+
+
+def write_ascii_beam(path: str, bunches: List[BeamBunch], new_file: bool = True, alive_only: bool = False):
+    cols = ["index", "vec", "p0c", "s_position", "time", "charge", "spin", "state", "ix_ele", "ix_branch",
+            "location", "species", "direction", "time_dir"]
+    # constant columns go to the header (the reference's remove_col rules)
+    const = {"charge": all(np.all(b.charge == b.charge[0]) for b in bunches if b.n),
+             "species": True, "ix_branch": True, "direction": True, "time_dir": True}
+    for k, c in const.items():
+        if c:
+            cols.remove(k)
+    with open(path, "w" if new_file else "a") as f:
+        for ib, b in enumerate(bunches, 1):
+            keep = np.ones(b.n, bool) if not alive_only else (b.state == 1) | (b.state == 0)
+            n_alive = int(np.sum((b.state == 1) | (b.state == 0)))
+            f.write(f"# ix_bunch       ={ib:6d}\n")
+            f.write(f"# n_particle     ={b.n:6d}\n")
+            f.write(f"# n_alive        ={n_alive:6d}\n")
+            f.write(f"# n_dead         ={b.n - n_alive:6d}\n")
+            # headwrite_re / _int / _str: the key tabbed to column 18
+            if "charge" not in cols:
+                f.write(_key("charge") + f"={(b.charge[0] if b.n else 0.0):24.16E}\n")
+            f.write(_key("ix_branch") + f"= {b.ix_branch}\n")
+            f.write(_key("direction") + f"= {b.direction}\n")
+            f.write(_key("time_dir") + f"= {b.time_dir}\n")
+            f.write(_key("species") + f"= {b.species}\n")
+            head = ""
+            for c in cols:
+                if c in ("index", "ix_ele"):
+                    head += f"{c:>8}"
+                elif c == "vec":
+                    head += "".join(f"{x:>23}" for x in ("x", "px", "y", "py", "z", "pz"))
+                elif c in ("p0c", "s_position", "time", "charge"):
+                    head += f"{c:>23}"
+                elif c == "spin":
+                    head += "".join(f"{x:>23}" for x in ("spin_x", "spin_y", "spin_z"))
+                elif c == "state":
+                    head += f"{c:>14}"
+                elif c == "location":
+                    head += f"{c:>16}"
+            f.write("#!" + head[2:] + "\n")
+            for ip in range(b.n):
+                if not keep[ip]:
+                    continue
+                row = ""
+                for c in cols:
+                    if c == "index":
+                        row += f"{ip + 1:8d}"
+                    elif c == "vec":
+                        row += "".join(_es(v) for v in b.vec6[:, ip])
+                    elif c == "p0c":
+                        row += _es(b.p0c[ip])
+                    elif c == "s_position":
+                        row += _es(b.s[ip])
+                    elif c == "time":
+                        row += _es(b.t[ip])
+                    elif c == "charge":
+                        row += _es(b.charge[ip])
+                    elif c == "spin":
+                        row += "".join(_es(v) for v in b.spin[:, ip])
+                    elif c == "state":
+                        row += f"{STATE_NAME[int(b.state[ip])]:>14}"
+                    elif c == "ix_ele":
+                        row += f"{int(b.ix_ele[ip]):8d}"
+                    elif c == "location":
+                        row += f"{b.location:>16}"
+                f.write(row.rstrip() + "\n")
+
+
+def _float(tok: str) -> float:
+    t = tok.strip().replace("D", "E").replace("d", "e")
+    try:
+        return float(t)
+    except ValueError:
+        # Fortran drops the 'E' for three-digit exponents: 1.0-100
+        for i in range(len(t) - 1, 0, -1):
+            if t[i] in "+-" and t[i - 1] not in "eE":
+                return float(t[:i] + "E" + t[i:])
+        raise
+
+
+def _match(name: str, table: List[str], what: str) -> int:
+    for i, s in enumerate(table):
+        if s.lower() == name.strip().strip("'\"").lower():
+            return i
+    raise ValueError(f"{what} name not recognised: {name!r}")
+
+
+def read_ascii_beam(path: str) -> List[BeamBunch]:
+    """Every bunch of an ASCII beam file."""
+    lines = open(path).read().splitlines()
+    out: List[BeamBunch] = []
+    i = 0
+    while i < len(lines):
+        hdr: Dict[str, str] = {}
+        cols: Optional[List[str]] = None
+        while i < len(lines):
+            ln = lines[i]
+            i += 1
+            if ln.strip() == "":
+                continue
+            if ln.startswith("#!"):
+                cols = ln[2:].split()
+                break
+            if not ln.startswith("#"):
+                raise ValueError(f"header line does not start with '#': {ln[:20]!r}")
+            if "=" in ln:
+                k, v = ln[1:].split("=", 1)
+                hdr[k.strip().lower()] = v.strip()
+        if cols is None:
+            break
+        rows = []
+        while i < len(lines):
+            ln = lines[i]
+            if ln.strip() == "":
+                i += 1
+                continue
+            if ln.startswith("#"):
+                break
+            rows.append(ln.split())
+            i += 1
+        n = len(rows)
+        species = hdr.get("species", "positron").strip("'\"")
+        p0 = {"p0c": _float(hdr["p0c"]) if "p0c" in hdr else 0.0,
+              "s": _float(hdr.get("s", hdr.get("s_position", "0"))), "t": _float(hdr.get("t", hdr.get("time", "0"))),
+              "charge": _float(hdr.get("charge", "0"))}
+        b = BeamBunch(np.zeros((6, n)), np.full(n, _match(hdr["state"], STATE_NAME, "state") if "state" in hdr
+                                                 else 1, np.int32),
+                      np.full(n, p0["p0c"]), np.full(n, p0["s"]), np.full(n, p0["t"]), np.full(n, p0["charge"]),
+                      np.zeros((3, n)), np.zeros(n, np.int32), None, species,
+                      hdr.get("location", "Downstream_End"), int(_float(hdr.get("ix_branch", "0"))),
+                      int(_float(hdr.get("direction", "1"))), int(_float(hdr.get("time_dir", "1"))),
+                      _float(hdr["charge_tot"]) if "charge_tot" in hdr else None)
+        if "beta" in hdr:
+            b.beta = np.full(n, _float(hdr["beta"]))
+        vec_idx = {"x": 0, "px": 1, "y": 2, "py": 3, "z": 4, "pz": 5}
+        spin_idx = {"spin_x": 0, "spin_y": 1, "spin_z": 2}
+        for ip, r in enumerate(rows):
+            if len(r) < len(cols):
+                raise ValueError(f"row {ip + 1} of a bunch has {len(r)} entries for {len(cols)} columns")
+            for c, tok in zip(cols, r):
+                cl = c.lower()
+                if cl in vec_idx:
+                    b.vec6[vec_idx[cl], ip] = _float(tok)
+                elif cl in spin_idx:
+                    b.spin[spin_idx[cl], ip] = _float(tok)
+                elif cl == "p0c":
+                    b.p0c[ip] = _float(tok)
+                elif cl in ("s", "s_position"):
+                    b.s[ip] = _float(tok)
+                elif cl in ("t", "time"):
+                    b.t[ip] = _float(tok)
+                elif cl == "charge":
+                    b.charge[ip] = _float(tok)
+                elif cl == "beta":
+                    if b.beta is None:
+                        b.beta = np.zeros(n)
+                    b.beta[ip] = _float(tok)
+                elif cl == "state":
+                    b.state[ip] = _match(tok, STATE_NAME, "state")
+                elif cl == "ix_ele":
+                    b.ix_ele[ip] = int(tok)
+                elif cl == "location":
+                    b.location = LOCATION_NAME[_match(tok, LOCATION_NAME, "location")]
+                elif cl == "species":
+                    b.species = tok
+                elif cl == "index":
+                    int(tok)  # must be an integer; value unused
+                elif cl in ("ix_branch", "direction", "time_dir", "ix_user"):
+                    int(tok)
+                elif cl in ("field_x", "field_y", "phase_x", "phase_y", "dt_ref", "r", "e_potential"):
+                    _float(tok)
+                else:
+                    raise ValueError(f"column name not recognised: {c}")
+        out.append(b)
+    return out
+
+
+def save_checkpoint(path: str, bunch: Bunch, next_turn: int, **meta):
+    """Exact tracker state and the index of the next turn to track."""
+    np.savez(path, vec6=bunch.vec6, beta=bunch.beta, state=bunch.state, ix_ele_lost=bunch.ix_ele_lost,
+             ix_turn_lost=bunch.ix_turn_lost, next_turn=np.int64(next_turn),
+             **{k: np.asarray(v) for k, v in meta.items()})
+
+
+def load_checkpoint(path: str):
+    """(Bunch, next_turn, meta) from save_checkpoint."""
+    z = np.load(path)
+    b = Bunch(np.ascontiguousarray(z["vec6"]), np.ascontiguousarray(z["beta"]), np.ascontiguousarray(z["state"]),
+              np.ascontiguousarray(z["ix_ele_lost"]), np.ascontiguousarray(z["ix_turn_lost"]))
+    meta = {k: z[k] for k in z.files if k not in ("vec6", "beta", "state", "ix_ele_lost", "ix_turn_lost",
+                                                   "next_turn")}
+    return b, int(z["next_turn"]), meta
