@@ -195,7 +195,9 @@ __device__ __forceinline__ void track_a_drift(Part& p, double length, const Glob
   if (p.beta > 0) {
     if (REF_MOTION) {
       double a = drift_pz_term(p, G, m);
-      dz = length * (a + sqrt_one(-pxy2) / ps_rel);
+      // sqrt_one(-pxy2) = -pxy2 / (sqrt(1 + (-pxy2)) + 1), and
+      // sqrt(1 + (-pxy2)) is ps_rel bit for bit (1 + (-a) == 1 - a)
+      dz = length * (a + (-pxy2 / (ps_rel + 1.0)) / ps_rel);
     } else {
       dz = -length / ps_rel;
     }
