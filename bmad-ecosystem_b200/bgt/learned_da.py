@@ -118,14 +118,30 @@ def grid_probes(pb: ScanProblem, v_begin: int, v_end: int, jitter_seed: Optional
     return torch.tensor(v6, device=dev).contiguous(), torch.tensor(var, device=dev)
 
 
-class _Bunch:
-    """Device particle arrays of a scan."""
+def tracking_order(pb: ScanProblem, nv: int):
+    """Probe index held by each tracking position: radius-major inside each
+    (variant, delta), so a warp tracks one radius across the angles and the
+    warps of a CTA are lost at similar turns (no idling at the end-of-tile
+    barrier).  Results do not depend on the order."""
+    import torch
 
-    def __init__(self, vec6, variant, p0c, mass):
+    idx = np.arange(nv * pb.per_variant).reshape(nv, len(pb.deltas), pb.n_angle, pb.n_radius)
+    return torch.tensor(idx.transpose(0, 1, 3, 2).ravel(), device=_device())
+
+
+class _Bunch:
+    """Device particle arrays of a scan, held in tracking order
+    (`order[k]` = probe index at tracking position k)."""
+
+    def __init__(self, vec6, variant, p0c, mass, order=None):
         import torch
 
-        self.vec = vec6.clone()
-        self.var = variant
+        self.order = order
+        if order is not None:
+            vec6 = vec6[:, order]
+            variant = variant[order]
+        self.vec = vec6.contiguous().clone()
+        self.var = variant.contiguous()
         n = vec6.shape[1]
         # beta as the one-launch scan computes it: pc / sqrt(pc^2 + m^2)
         pc = (1 + vec6[5]) * p0c
@@ -134,8 +150,19 @@ class _Bunch:
         self.ixe = torch.full((n,), -1, dtype=torch.int32, device=vec6.device)
         self.ixt = torch.full((n,), -1, dtype=torch.int32, device=vec6.device)
 
+    def probe_order(self, t):
+        """A tracking-order array (last axis) in probe order."""
+        import torch
+
+        if self.order is None:
+            return t
+        out = torch.empty_like(t)
+        out[..., self.order] = t
+        return out
+
     def subset(self, idx):
         b = _Bunch.__new__(_Bunch)
+        b.order = None
         b.vec = self.vec[:, idx].contiguous()
         b.beta = self.beta[idx].contiguous()
         b.state = self.state[idx].contiguous()
@@ -180,12 +207,12 @@ def staged_scan(pb: ScanProblem, v_begin: int, v_end: int, early: int = 64, n_tu
     t0 = time.perf_counter()
     vec0, var = grid_probes(pb, v_begin, v_end, jitter_seed)
     tr = pb.tracker
-    b = _Bunch(vec0, var, tr.p0c, tr.species.mass)
+    b = _Bunch(vec0, var, tr.p0c, tr.species.mass, tracking_order(pb, v_end - v_begin))
     b.track(tr, early, 0)
-    snap = b.vec.clone()
-    alive = b.state == 1
+    snap = b.probe_order(b.vec)
+    alive = b.probe_order(b.state) == 1
     b.track(tr, nt - early, early)
-    surv = survive_turns(b.state, b.ixt, nt)
+    surv = b.probe_order(survive_turns(b.state, b.ixt, nt))
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     pt = int(torch.clamp(surv, max=nt).sum().item())
@@ -272,11 +299,11 @@ def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, ear
     t0 = time.perf_counter()
     vec0, var = grid_probes(pb, v_begin, v_end)
     tr = pb.tracker
-    b = _Bunch(vec0, var, tr.p0c, tr.species.mass)
+    b = _Bunch(vec0, var, tr.p0c, tr.species.mass, tracking_order(pb, nv))
     b.track(tr, early, 0)
-    alive = b.state == 1
+    alive = b.probe_order(b.state) == 1
     table = torch.tensor(pb.table, device=dev)
-    x, _ = net.features(vec0, b.vec, var, table)
+    x, _ = net.features(vec0, b.probe_order(b.vec).contiguous(), var, table)
     n = vec0.shape[1]
     p = net.forward(x)[:n]
     # predicted DA boundary of each ray: the first probe lost or predicted lost
@@ -290,7 +317,8 @@ def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, ear
     gen = torch.Generator(device="cpu").manual_seed(seed)
     aud = (torch.rand(n, generator=gen) < audit).to(dev)
     track_mask = alive & (band | near | aud)
-    idx = torch.nonzero(track_mask).view(-1)  # ascending: variants stay sorted
+    # tracking positions of the kept probes, ascending: variants stay sorted
+    idx = torch.nonzero(track_mask[b.order]).view(-1)
     m = int(idx.numel())
     label = torch.where(alive, p <= 0.5, torch.zeros_like(alive))
     actual = label.clone()
@@ -298,7 +326,7 @@ def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, ear
     if m:
         sub = b.subset(idx)
         sub.track(tr, nt - early, early)
-        actual[idx] = sub.state == 1
+        actual[b.order[idx]] = sub.state == 1
         tracked_turns = int((survive_turns(sub.state, sub.ixt, nt) - early).clamp(min=0).sum().item())
     early_turns = int(torch.clamp(survive_turns(b.state, b.ixt, early), max=early).sum().item())
     torch.cuda.synchronize()

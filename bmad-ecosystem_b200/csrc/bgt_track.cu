@@ -1791,8 +1791,12 @@ __global__ void da_init_kernel(DAArgs A, int64_t n) {
   A.state[i] = ALIVE;
   A.ixe[i] = -1;
   A.ixt[i] = -1;
-  // slot of this particle: variant-major, padded per variant
-  int64_t within = i - (int64_t)v * A.per_var;
+  // slot of this particle: variant-major, padded per variant; inside a
+  // variant radius-major ((d * n_radius + r) * n_angle + a), so that a warp
+  // (and a CTA) holds probes of one or few radii across the angles -- they
+  // are lost at similar turns, and warps of a CTA finish together instead of
+  // idling at the end-of-tile barrier.  Results do not depend on the slot.
+  int64_t within = ((int64_t)d * A.n_radius + r) * A.n_angle + a;
   A.slot[(int64_t)v * A.slots_per_var + within] = (int32_t)i;
 }
 

@@ -146,3 +146,18 @@ def test_error_variant_ring_matches_oracle():
         tr.track_turns(b, 20)
         assert np.array_equal(b.vec6, ov) and np.array_equal(b.state, ost)
         assert np.array_equal(b.ix_ele_lost, oie) and np.array_equal(b.ix_turn_lost, oit)
+
+
+def test_staged_scan_equals_one_launch_scan(variants):
+    """The Python driver's two-launch scan (turn-64 snapshot, radius-major
+    tracking order) gives the one-launch scan's survival turns exactly."""
+    from bgt import da, rings
+    from bgt import learned_da as LD
+    from bgt.track import Tracker
+
+    grid = rings.DAGrid(6, 16, 0.03, (-0.01, 0.0), 90)
+    pb = LD.setup(Tracker(variants), variants, grid)
+    st = LD.staged_scan(pb, 0, 3, early=20)
+    plain = da.plain_scan(pb.tracker, pb.ref, **pb.grid())
+    assert np.array_equal(st.survive.cpu().numpy(), plain.survive_turns.reshape(-1))
+    assert np.any(plain.survive_turns < 90) and np.any(plain.survive_turns == 90)
