@@ -577,6 +577,80 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
   const QMemo qmemo{qmemo_base + threadIdx.x, BLOCK};
 
   const int tid = threadIdx.x;
+  if (GTAB) {
+    // Tables in global memory: no CTA-wide state to share, so every warp
+    // runs its own persistent loop over 32-slot tiles and never waits at a
+    // CTA barrier for warps whose particles live longer (DA scans mix
+    // short- and long-lived probes in one tile).  No compaction here.
+    const int lane = tid & 31;
+    const int64_t n_wtiles = (a.n_slots + 31) / 32;
+    while (true) {
+      int64_t wt = 0;
+      if (lane == 0) wt = atomicAdd(a.tile_counter, 1);
+      wt = __shfl_sync(0xffffffffu, wt, 0);
+      if (wt >= n_wtiles) break;
+      const int64_t slot = wt * 32 + lane;
+      // slots are grouped per variant in multiples of the CTA size, so the
+      // 32 slots of a warp tile share one variant
+      const int variant = a.tile_variant ? a.tile_variant[(wt * 32) / BLOCK] : 0;
+      const double* wtable = a.tables + a.table_off_dw[variant];
+      const int2* wseq = reinterpret_cast<const int2*>(wtable);
+      int64_t pidx = -1;
+      if (slot < a.n_slots) pidx = a.slot_particle ? a.slot_particle[slot] : slot;
+      if (pidx >= a.n) pidx = -1;
+      Part p;
+      int32_t ixe = -1, ixt = -1;
+      p.state = 0;
+      if (pidx >= 0) {
+        p.x = a.vec6[0 * a.n_stride + pidx];
+        p.px = a.vec6[1 * a.n_stride + pidx];
+        p.y = a.vec6[2 * a.n_stride + pidx];
+        p.py = a.vec6[3 * a.n_stride + pidx];
+        p.z = a.vec6[4 * a.n_stride + pidx];
+        p.pz = a.vec6[5 * a.n_stride + pidx];
+        p.beta = a.beta[pidx];
+        p.state = a.state[pidx];
+        ixe = a.ix_ele_lost[pidx];
+        if (a.ix_turn_lost) ixt = a.ix_turn_lost[pidx];
+      }
+      DriftMemo memo;
+      memo.pz = NAN;
+      memo.a = 0;
+#pragma unroll
+      for (int c = 0; c < QMEMO_CLASSES; c++) qmemo.q[(c * 13 + 12) * qmemo.stride] = NAN;
+      if (p.state == ALIVE && orbit_too_large(p, a.G)) {
+        ixe = wseq[a.rec_begin].y;
+        ixt = a.turn0;
+      }
+      for (int t = 0; t < a.n_turns; t++) {
+        if (__all_sync(0xffffffffu, p.state != ALIVE)) break;  // whole warp lost
+        const int turn = a.turn0 + t;
+        for (int r = a.rec_begin; r < a.rec_end; r++) {
+          const int2 e = wseq[r];
+          if (p.state == ALIVE) {
+            track1_rec(p, wtable + e.x, a.G, memo, qmemo);
+            if (p.state != ALIVE) {
+              ixe = e.y;
+              ixt = turn;
+            }
+          }
+        }
+      }
+      if (pidx >= 0) {
+        a.vec6[0 * a.n_stride + pidx] = p.x;
+        a.vec6[1 * a.n_stride + pidx] = p.px;
+        a.vec6[2 * a.n_stride + pidx] = p.y;
+        a.vec6[3 * a.n_stride + pidx] = p.py;
+        a.vec6[4 * a.n_stride + pidx] = p.z;
+        a.vec6[5 * a.n_stride + pidx] = p.pz;
+        a.beta[pidx] = p.beta;
+        a.state[pidx] = p.state;
+        a.ix_ele_lost[pidx] = ixe;
+        if (a.ix_turn_lost) a.ix_turn_lost[pidx] = ixt;
+      }
+    }
+    return;
+  }
   if (tid == 0) mbar_init(&bar, 1);
   __syncthreads();
   uint32_t parity = 0;
