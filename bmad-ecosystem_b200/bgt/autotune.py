@@ -25,7 +25,7 @@ SHAPES: Tuple[Tuple[int, int], ...] = ((64, 8), (64, 10), (64, 12), (64, 16), (1
                                        (128, 8), (256, 2), (256, 3), (256, 4))
 
 # shapes compiled with the element table read from global memory (table_mode 2)
-GLOBAL_TABLE_SHAPES: Tuple[Tuple[int, int], ...] = ((128, 4), (128, 5), (256, 2), (256, 3))
+GLOBAL_TABLE_SHAPES: Tuple[Tuple[int, int], ...] = ((128, 3), (128, 4), (128, 5), (256, 2), (256, 3))
 
 _cache: Dict[str, dict] = {}
 
@@ -86,8 +86,11 @@ def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, 
     beta0 = pc / torch.sqrt(pc * pc + tracker.species.mass ** 2)
     stream = torch.cuda.current_stream(dev)
     results = []
+    shapes = list(shapes)
     cands = [(tpb, bps, ce, tm) for (tpb, bps) in shapes for ce in compact_options
              for tm in ((0, 2) if (tpb, bps) in GLOBAL_TABLE_SHAPES else (0,))]
+    # shapes compiled only for global-memory tables
+    cands += [(tpb, bps, 0, 2) for (tpb, bps) in GLOBAL_TABLE_SHAPES if (tpb, bps) not in shapes]
     for (tpb, bps, ce, tm) in cands:
         tun = dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0, table_mode=tm)
         tracker.set_tuning(**tun)

@@ -288,7 +288,12 @@ class PrunedResult:
 
 def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, early: int = 64,
                 n_turns: Optional[int] = None, p_hi: float = 0.98, p_lo: float = 0.02, audit: float = 0.02,
-                boundary_cells: int = 2, seed: int = 0) -> PrunedResult:
+                boundary_cells: int = 2, seed: int = 0, retune_subset: bool = True) -> PrunedResult:
+    """The kept probes are far fewer than the grid, so their tracking is
+    bound by one particle's turn latency rather than by throughput; with
+    `retune_subset` the launch shape for them is re-tuned on the kept set
+    itself (a few 2-turn trial launches) and the scan's tuning restored
+    afterwards."""
     import torch
 
     nt = pb.n_turns if n_turns is None else n_turns
@@ -325,7 +330,13 @@ def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, ear
     tracked_turns = 0
     if m:
         sub = b.subset(idx)
+        saved = tr.get_tuning()
+        if retune_subset:
+            from . import autotune
+
+            autotune.tune(tr, sub.vec.cpu().numpy(), turns=2, sample=m, variant=sub.var.cpu().numpy())
         sub.track(tr, nt - early, early)
+        tr.set_tuning(**saved)
         actual[b.order[idx]] = sub.state == 1
         tracked_turns = int((survive_turns(sub.state, sub.ixt, nt) - early).clamp(min=0).sum().item())
     early_turns = int(torch.clamp(survive_turns(b.state, b.ixt, early), max=early).sum().item())

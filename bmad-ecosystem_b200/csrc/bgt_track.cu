@@ -1407,13 +1407,16 @@ static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t s
   const int bps = h->tuning.blocks_per_sm;
   if (gtab) {
     switch (block * 100 + bps) {
+      // (128, 3): 170 registers per thread, no spills -- for small,
+      // long-lived sets where one particle's turn latency sets the time
+      case 12803: e = launch_track<128, 3, true>(a, (int)grid, smem, st); break;
       case 12804: e = launch_track<128, 4, true>(a, (int)grid, smem, st); break;
       case 12805: e = launch_track<128, 5, true>(a, (int)grid, smem, st); break;
       case 25602: e = launch_track<256, 2, true>(a, (int)grid, smem, st); break;
       case 25603: e = launch_track<256, 3, true>(a, (int)grid, smem, st); break;
       default:
         return set_err(h, BGT_ETOOLARGE,
-                       "element table read from global memory: tuning must be (128: 4,5) or (256: 2,3)");
+                       "element table read from global memory: tuning must be (128: 3,4,5) or (256: 2,3)");
     }
     if (e != cudaSuccess)
       return set_err(h, BGT_ECUDA, std::string("track_kernel launch: ") + cudaGetErrorString(e));
