@@ -455,6 +455,71 @@ __device__ __forceinline__ void apply_energy_kick(Part& p, double dE, const Glob
   p.beta = beta_new;
 }
 
+// Electric multipole kicks: ab_multipole_kicks with electric = true
+// (bmad/modules/multipole_mod.f90:82-174, ab_multipole_kick :314-401):
+// kick factor charge / (beta p0c) per order (b enters with a minus sign),
+// then the energy change from the transverse kick: pz, beta and z rescaled.
+__device__ __forceinline__ void ab_multipole_kicks_elec(Part& p, const double* ae, const double* be, int ix_max,
+                                                        double scale, const Glob& G) {
+  const double px0 = p.px, py0 = p.py, pz0 = p.pz, z0 = p.z, beta0 = p.beta;
+  const double x = p.x, y = p.y;
+  double kx_tot = 0, ky_tot = 0;
+  for (int n = 0; n <= ix_max; n++) {
+    const double a = ae[n], b = be[n];
+    double kx = 0, ky = 0;
+    if (!(a == 0 && b == 0)) {
+      const double f = (double)G.charge / (p.beta * G.p0c);
+      double a2 = a * f, b2 = -b * f;
+      a2 = scale * a2;
+      b2 = scale * b2;
+      for (int m = 0; m <= n; m += 2) {
+        const double t = c_cm[n][m] * mexp_d(x, n - m) * mexp_d(y, m);
+        kx = kx + b2 * t;
+        ky = ky - a2 * t;
+      }
+      for (int m = 1; m <= n; m += 2) {
+        const double t = c_cm[n][m] * mexp_d(x, n - m) * mexp_d(y, m);
+        kx = kx + a2 * t;
+        ky = ky + b2 * t;
+      }
+    }
+    kx_tot = kx_tot + kx;
+    ky_tot = ky_tot + ky;
+  }
+  p.px = p.px + kx_tot;
+  p.py = p.py + ky_tot;
+  const double alpha = (kx_tot * (2 * px0 + kx_tot) + ky_tot * (2 * py0 + ky_tot)) / sq(1 + pz0);
+  if (alpha < -1) {
+    p.state = LOST_PZ;
+    return;
+  }
+  const double dpz = (1 + pz0) * sqrt_one(alpha);
+  p.pz = pz0 + dpz;
+  p.beta = (1 + p.pz) / sqrt(sq(1 + p.pz) + sq(G.mc2 / G.p0c));
+  p.z = z0 * p.beta / beta0;
+}
+
+// electric_longitudinal_fringe, bmad/low_level/apply_element_edge_kick.f90:
+// 283-329: the energy change crossing the edge of the electric multipole
+// potential; at_sign +1 entering, -1 leaving (the element has length).
+__device__ __forceinline__ void electric_longitudinal_fringe(Part& p, const double* ae, const double* be, int ix_max,
+                                                             double at_sign, const Glob& G) {
+  const double ff = at_sign * (double)G.charge;
+  double xr = 1, xi = 0;
+  const double cr = p.x, ci = p.y;
+  double phi = 0;
+  for (int i = 0; i <= ix_max; i++) {
+    const double nr = xr * cr - xi * ci;
+    const double ni = xr * ci + xi * cr;
+    xr = nr;
+    xi = ni;
+    if (ae[i] == 0 && be[i] == 0) continue;
+    const double abr = be[i], abi = -ae[i];
+    phi = phi - (abr * xr - abi * xi) / (i + 1);
+  }
+  apply_energy_kick(p, -ff * phi, G);
+}
+
 // ---------------------------------------------------------------------------
 // Hwang hard-edge bend fringe, bmad/modules/fringe_mod.f90:240-418 (td = +1)
 template <bool ENTERING>

@@ -42,6 +42,13 @@ enum Flag : int32_t {
   F_K1_BODY = 1 << 12,     // bend: sbend_body_with_k1_map
   F_DRIFT_BODY = 1 << 13,  // bend: body is a plain drift (g == dg == 0 or step_len == 0)
   F_IS_OFF = 1 << 14,      // bend is off (is_on = F)
+  // quadrupole / thick multipole: init_fringe_info is true (a fringe type or
+  // electric multipoles): the state is checked after each edge kick
+  F_FRINGE_INFO = 1 << 15,
+  // quadrupole / thick multipole: electric multipoles, ae[aux1+1] and
+  // be[aux1+1] follow the magnetic an/bn arrays; F_EDGE_IN / F_EDGE_OUT then
+  // mark the ends with an electric longitudinal fringe kick
+  F_ELEC = 1 << 16,
 };
 
 struct RecHdr {

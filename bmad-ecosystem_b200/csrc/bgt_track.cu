@@ -69,16 +69,25 @@ struct QMemo {
   int stride;
 };
 
-// bmad/low_level/track_a_quadrupole.f90:134-265 (magnetic, no fringe)
+// bmad/low_level/track_a_quadrupole.f90:134-265 (magnetic and electric
+// multipoles; no quadrupole fringe)
 __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, DriftMemo& m, QMemo qm) {
   const double* q = R.kb;
   const int32_t fl = R.h->flags;
   const int ix = R.h->ix_mag_max;
+  const int ixe = R.h->aux1;
   const int n_step = R.h->n_step;
   const double* an = q + Q_N;
   const double* bn = an + (ix + 1);
+  const double* ae = an + 2 * (ix + 1);
+  const double* be = ae + (ixe + 1);
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
+  if (fl & F_FRINGE_INFO) {
+    if (fl & F_EDGE_IN) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+    if (p.state != ALIVE) return;
+  }
   if (ix > -1) ab_multipole_kicks(p, an, bn, ix, q[Q_RHALF]);
+  if (ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, q[Q_STEP] / 2, G);
   const double step = q[Q_STEP];
   // rel_p changes only through electric fields, absent here: quad_mat2_calc
   // has identical inputs at every step, so it is evaluated once.
@@ -116,6 +125,11 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
     p.py = my.m10 * y + my.cx * py;
     p.z = p.z + low_energy_z_correction(p, q + Q_LEZ, step);
     if (ix > -1) ab_multipole_kicks(p, an, bn, ix, (i == n_step) ? q[Q_RHALF] : q[Q_RSTEP]);
+    if (ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, (i == n_step) ? q[Q_STEP] / 2 : q[Q_STEP], G);
+  }
+  if (fl & F_FRINGE_INFO) {
+    if (fl & F_EDGE_OUT) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+    if (p.state != ALIVE) return;
   }
   if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
 }
@@ -126,13 +140,26 @@ __device__ __forceinline__ void body_thick(Part& p, const Rec& R, const Glob& G,
   const int32_t fl = R.h->flags;
   const int ix = R.h->ix_mag_max;
   const int n_step = R.h->n_step;
+  const int ixe = R.h->aux1;
   const double* an = q + TM_N;
   const double* bn = an + (ix + 1);
+  const double* ae = an + 2 * (ix + 1);
+  const double* be = ae + (ixe + 1);
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
+  if (fl & F_FRINGE_INFO) {
+    if (fl & F_EDGE_IN) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+    if (p.state != ALIVE) return;
+  }
   if (ix > -1) ab_multipole_kicks(p, an, bn, ix, q[TM_RHALF]);
+  if (ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, q[TM_STEP] / 2, G);
   for (int i = 1; i <= n_step; i++) {
     track_a_drift<true>(p, q[TM_STEP], G, m);
     if (ix > -1) ab_multipole_kicks(p, an, bn, ix, (i == n_step) ? q[TM_RHALF] : q[TM_RSTEP]);
+    if (ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, (i == n_step) ? q[TM_STEP] / 2 : q[TM_STEP], G);
+  }
+  if (fl & F_FRINGE_INFO) {
+    if (fl & F_EDGE_OUT) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+    if (p.state != ALIVE) return;
   }
   if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
 }
@@ -940,11 +967,11 @@ static void put_edge(double* E, const bgt_element& e, bool entering) {
 // Compile one element into a record.  Returns 0 or BGT_EUNSUPPORTED with err set.
 static int compile_element(const bgt_element& e, const bgt_species& sp, double p0c, std::vector<double>& out,
                            std::string& err) {
-  for (int n = 0; n < BGT_N_POLE; n++) {
-    if (e.an_elec[n] != 0 || e.bn_elec[n] != 0) {
-      err = ename(e) + ": electric multipoles are not supported";
-      return BGT_EUNSUPPORTED;
-    }
+  const int ixe = max_nonzero(e.an_elec, e.bn_elec, BGT_N_POLE);
+  if (ixe > -1 && e.is_on && e.key != BGT_QUADRUPOLE && e.key != BGT_SEXTUPOLE && e.key != BGT_OCTUPOLE &&
+      e.key != BGT_THICK_MULTIPOLE) {
+    err = ename(e) + ": electric multipoles are supported on quadrupoles and thick multipoles only";
+    return BGT_EUNSUPPORTED;
   }
   if (e.p0c != p0c) {
     err = ename(e) + ": element p0c differs from the lattice reference momentum";
@@ -1103,7 +1130,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       if (ix <= 1) ix = max_nonzero(an, bn, 2);
       double length = 1 * e.l;
       int n_step = 1;
-      if (ix > -1) n_step = std::max(nint_h(fabs(length) / e.ds_step), 1);
+      if (ix > -1 || ixe > -1) n_step = std::max(nint_h(fabs(length) / e.ds_step), 1);
       double r_step = 1.0 / n_step;
       double step_len = e.l * r_step;
       if (length == 0) n_step = 0;
@@ -1128,7 +1155,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       }
       if (key == BGT_PIPE) ix = -1;  // multipole_ele_to_ab returns nothing for pipes
       double length = e.l * 1;
-      int n_step = (ix == -1) ? 1 : std::max(nint_h(fabs(length / e.ds_step)), 1);
+      int n_step = (ix == -1 && ixe == -1) ? 1 : std::max(nint_h(fabs(length / e.ds_step)), 1);
       double r_step = 1.0 / n_step;
       double step_len = length / n_step;
       double* q = B.ptr_after_push(TM_N);
@@ -1276,6 +1303,27 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     for (int n = 0; n <= ix; n++) {
       q[n] = an[n];
       q[ix + 1 + n] = bn[n];
+    }
+  }
+  h.aux1 = -1;
+  if (kind == K_QUAD || kind == K_THICK_MULT) {
+    // init_fringe_info (bmad/low_level/init_fringe_info.f90:22-60)
+    const bool fringe = (e.fringe_type != BGT_FRINGE_NONE && e.fringe_at != BGT_NO_END) || ixe > -1;
+    if (fringe) flags |= F_FRINGE_INFO;
+    if (ixe > -1) {
+      flags |= F_ELEC;
+      h.aux1 = ixe;
+      double* q = B.ptr_after_push(2 * (ixe + 1));
+      for (int n = 0; n <= ixe; n++) {
+        q[n] = e.an_elec[n];
+        q[ixe + 1 + n] = e.bn_elec[n];
+      }
+      // electric_longitudinal_fringe (apply_element_edge_kick.f90:283-329)
+      // acts at the ends fringe_at names, and not at all for zero length
+      if (e.l != 0) {
+        if (e.fringe_at == BGT_ENTRANCE_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_IN;
+        if (e.fringe_at == BGT_EXIT_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_OUT;
+      }
     }
   }
   h.flags = flags;
