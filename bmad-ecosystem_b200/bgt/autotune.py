@@ -24,7 +24,7 @@ from . import _lib
 SHAPES: Tuple[Tuple[int, int], ...] = ((64, 8), (64, 10), (64, 12), (64, 16), (128, 4), (128, 5), (128, 6),
                                        (128, 8), (256, 2), (256, 3), (256, 4))
 
-# shapes compiled with the element table read from global memory (table_mode 2)
+# shapes compiled with the element table read from global memory (table_mode 2 and 3)
 GLOBAL_TABLE_SHAPES: Tuple[Tuple[int, int], ...] = ((128, 3), (128, 4), (128, 5), (256, 2), (256, 3))
 
 _cache: Dict[str, dict] = {}
@@ -88,9 +88,9 @@ def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, 
     results = []
     shapes = list(shapes)
     cands = [(tpb, bps, ce, tm) for (tpb, bps) in shapes for ce in compact_options
-             for tm in ((0, 2) if (tpb, bps) in GLOBAL_TABLE_SHAPES else (0,))]
+             for tm in ((0, 2, 3) if (tpb, bps) in GLOBAL_TABLE_SHAPES else (0,))]
     # shapes compiled only for global-memory tables
-    cands += [(tpb, bps, 0, 2) for (tpb, bps) in GLOBAL_TABLE_SHAPES if (tpb, bps) not in shapes]
+    cands += [(tpb, bps, 0, tm) for (tpb, bps) in GLOBAL_TABLE_SHAPES if (tpb, bps) not in shapes for tm in (2, 3)]
     for (tpb, bps, ce, tm) in cands:
         tun = dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0, table_mode=tm)
         tracker.set_tuning(**tun)

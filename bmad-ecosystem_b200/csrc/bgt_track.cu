@@ -584,13 +584,15 @@ struct KArgs {
 
 constexpr int MAX_BLOCK = 256;
 
-// GTAB: the variant's element table is read from global memory (L2 / L1)
-// instead of being staged in shared memory -- for tables larger than the
-// shared-memory budget (e.g. every quadrupole and sextupole misaligned and
-// carrying its own multipole errors), or to leave shared memory to more
-// resident CTAs.
-template <int BLOCK, int MINB, bool GTAB>
+// TMODE 0: the variant's element table is staged in shared memory.
+// TMODE 1: it is read from global memory (L2 / L1) instead -- for tables
+//   larger than the shared-memory budget (e.g. every quadrupole and sextupole
+//   misaligned and carrying its own multipole errors), or to leave shared
+//   memory to more resident CTAs; CTA-wide tiles as in TMODE 0.
+// TMODE 2: global-memory tables with every warp scheduled on its own.
+template <int BLOCK, int MINB, int TMODE>
 __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
+  constexpr bool GTAB = TMODE != 0;
   extern __shared__ __align__(128) double smem[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int32_t s_tile;
@@ -604,7 +606,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
   const QMemo qmemo{qmemo_base + threadIdx.x, BLOCK};
 
   const int tid = threadIdx.x;
-  if (GTAB) {
+  if (TMODE == 2) {
     // Tables in global memory: no CTA-wide state to share, so every warp
     // runs its own persistent loop over 32-slot tiles and never waits at a
     // CTA barrier for warps whose particles live longer (DA scans mix
@@ -1418,18 +1420,18 @@ static size_t smem_bytes(const bgt_handle* h, int block, bool compact, bool gtab
   return b;
 }
 
-template <int BLOCK, int MINB, bool GTAB = false>
+template <int BLOCK, int MINB, int TMODE = 0>
 static cudaError_t launch_track(const KArgs& a, int grid, size_t smem, cudaStream_t st) {
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK, MINB, GTAB>,
+    cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK, MINB, TMODE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     if (e != cudaSuccess) return e;
     attr_set[dev & 63] = true;
   }
-  track_kernel<BLOCK, MINB, GTAB><<<grid, BLOCK, smem, st>>>(a);
+  track_kernel<BLOCK, MINB, TMODE><<<grid, BLOCK, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1440,7 +1442,8 @@ static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t s
   const bool fits = smem_bytes(h, block, compact) <= SMEM_LIMIT;
   if (h->tuning.table_mode == 1 && !fits)
     return set_err(h, BGT_ETOOLARGE, "element table does not fit in shared memory (table_mode 1)");
-  const bool gtab = h->tuning.table_mode == 2 || !fits;
+  const bool gtab = h->tuning.table_mode >= 2 || !fits;
+  const bool warp_sched = h->tuning.table_mode == 3;
   size_t smem = smem_bytes(h, block, compact, gtab);
   if (smem > SMEM_LIMIT) return set_err(h, BGT_ETOOLARGE, "tracking state does not fit in shared memory");
   int64_t grid = (int64_t)h->num_sms * std::max(1, h->tuning.blocks_per_sm);
@@ -1454,14 +1457,19 @@ static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t s
   // __launch_bounds__, i.e. register caps of 128, 102, 85 and 64 per thread
   const int bps = h->tuning.blocks_per_sm;
   if (gtab) {
-    switch (block * 100 + bps) {
-      // (128, 3): 170 registers per thread, no spills -- for small,
-      // long-lived sets where one particle's turn latency sets the time
-      case 12803: e = launch_track<128, 3, true>(a, (int)grid, smem, st); break;
-      case 12804: e = launch_track<128, 4, true>(a, (int)grid, smem, st); break;
-      case 12805: e = launch_track<128, 5, true>(a, (int)grid, smem, st); break;
-      case 25602: e = launch_track<256, 2, true>(a, (int)grid, smem, st); break;
-      case 25603: e = launch_track<256, 3, true>(a, (int)grid, smem, st); break;
+    // (128, 3): 170 registers per thread, no spills -- for small,
+    // long-lived sets where one particle's turn latency sets the time
+    switch ((block * 100 + bps) * 10 + (warp_sched ? 2 : 1)) {
+      case 128031: e = launch_track<128, 3, 1>(a, (int)grid, smem, st); break;
+      case 128041: e = launch_track<128, 4, 1>(a, (int)grid, smem, st); break;
+      case 128051: e = launch_track<128, 5, 1>(a, (int)grid, smem, st); break;
+      case 256021: e = launch_track<256, 2, 1>(a, (int)grid, smem, st); break;
+      case 256031: e = launch_track<256, 3, 1>(a, (int)grid, smem, st); break;
+      case 128032: e = launch_track<128, 3, 2>(a, (int)grid, smem, st); break;
+      case 128042: e = launch_track<128, 4, 2>(a, (int)grid, smem, st); break;
+      case 128052: e = launch_track<128, 5, 2>(a, (int)grid, smem, st); break;
+      case 256022: e = launch_track<256, 2, 2>(a, (int)grid, smem, st); break;
+      case 256032: e = launch_track<256, 3, 2>(a, (int)grid, smem, st); break;
       default:
         return set_err(h, BGT_ETOOLARGE,
                        "element table read from global memory: tuning must be (128: 3,4,5) or (256: 2,3)");
@@ -1639,7 +1647,7 @@ int bgt_set_tuning(bgt_handle* h, const bgt_tuning* t) {
   if (n.threads_per_block != 64 && n.threads_per_block != 128 && n.threads_per_block != 256)
     return set_err(h, BGT_EINVAL, "threads_per_block must be 64, 128 or 256");
   if (n.compact_every < 0 || n.turns_per_launch < 0) return set_err(h, BGT_EINVAL, "negative tuning value");
-  if (n.table_mode < 0 || n.table_mode > 2) return set_err(h, BGT_EINVAL, "table_mode must be 0, 1 or 2");
+  if (n.table_mode < 0 || n.table_mode > 3) return set_err(h, BGT_EINVAL, "table_mode must be 0, 1, 2 or 3");
   h->tuning = n;
   return 0;
 }

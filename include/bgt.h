@@ -145,7 +145,9 @@ typedef struct bgt_tuning {
   int32_t turns_per_launch;  /* turns per persistent-kernel launch (graph node) */
   int32_t compact_every;     /* compact lost particles every this many turns (0 = never) */
   int32_t table_mode;        /* element table: 0 = staged in shared memory when it fits, else read
-                                from global memory; 1 = shared memory only; 2 = global memory */
+                                from global memory; 1 = shared memory only; 2 = global memory;
+                                3 = global memory with every warp scheduled on its own (no
+                                CTA-wide tiles: for small, long-lived particle sets) */
 } bgt_tuning;
 
 typedef struct bgt_handle bgt_handle;

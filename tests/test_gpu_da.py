@@ -105,11 +105,12 @@ def _two_error_rings():
     return L.Lattice(els, a.species, a.p0c, a.e_tot, "two_error_rings").finalize()
 
 
-@pytest.mark.parametrize("mode", ["auto", "global"])
+@pytest.mark.parametrize("mode", ["auto", "global", "global-warp"])
 def test_large_table_global_memory_path(mode):
     """Element tables too large for shared memory are read from global memory
-    (table_mode 0 picks it, 2 forces it); results stay bit-identical to the
-    correctly rounded oracle, and table_mode 1 refuses such a table."""
+    (table_mode 0 picks it, 2 forces it, 3 with per-warp scheduling); results
+    stay bit-identical to the correctly rounded oracle, and table_mode 1
+    refuses such a table."""
     from bgt import _lib, rings
     from bgt.track import Tracker
     from helpers import oracle_track_elements
@@ -117,7 +118,7 @@ def test_large_table_global_memory_path(mode):
     lat = _two_error_rings()
     tr = Tracker(lat)
     assert tr.table_bytes() > 224 * 1024
-    tr.set_tuning(threads_per_block=256, blocks_per_sm=2, table_mode=2 if mode == "global" else 0)
+    tr.set_tuning(threads_per_block=256, blocks_per_sm=2, table_mode={"auto": 0, "global": 2, "global-warp": 3}[mode])
     v0 = rings.gaussian_beam(rings.CONFIG1_BEAM, n=1024)
     b = tr.make_bunch(v0.copy())
     tr.track_turns(b, 3)
@@ -131,7 +132,7 @@ def test_large_table_global_memory_path(mode):
 def test_error_variant_ring_matches_oracle():
     """A full error-variant ring (every quadrupole with 16 kick-drift steps
     and multipoles b3..b6 / a3..a6, offsets and rolls) over 20 turns:
-    bit-identical to the correctly rounded oracle, in both table modes."""
+    bit-identical to the correctly rounded oracle, in every table mode."""
     from bgt import rings
     from bgt.track import Tracker
     from helpers import oracle_track_elements
@@ -140,7 +141,7 @@ def test_error_variant_ring_matches_oracle():
     v0 = rings.gaussian_beam(rings.CONFIG1_BEAM, n=2048)
     ov, _, ost, oie, oit = oracle_track_elements(lat, v0.copy(), 0, len(lat), n_turns=20, variant="cr")
     tr = Tracker(lat)
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         tr.set_tuning(threads_per_block=128, blocks_per_sm=4, table_mode=mode)
         b = tr.make_bunch(v0.copy())
         tr.track_turns(b, 20)
