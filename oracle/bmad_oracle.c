@@ -1275,6 +1275,79 @@ static void electric_longitudinal_fringe(bgo_coord* orb, const bgo_ele* ele, con
   apply_energy_kick(-ff * phi, orb, param);
 }
 
+/* hard_multipole_edge_kick, bmad/modules/fringe_mod.f90:691-864, tracking
+ * part (no matrix): the hard-edge fringe of the quadrupole (n = 1, k1) or
+ * sextupole (n = 2, k2) body field; charge_dir = 1 (forward tracking of the
+ * reference species).  Complex products are written out as gfortran forms
+ * them: (a + ib)(c + id) = (ac - bd) + i(ad + bc). */
+typedef struct {
+  double re, im;
+} bgo_cplx;
+static bgo_cplx cmul(bgo_cplx a, bgo_cplx b) {
+  bgo_cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+  FL(6);
+  return r;
+}
+static bgo_cplx cadd(bgo_cplx a, bgo_cplx b) {
+  bgo_cplx r = {a.re + b.re, a.im + b.im};
+  FL(2);
+  return r;
+}
+
+static void hard_multipole_edge_kick(const bgo_ele* ele, int first_edge, bgo_coord* orb) {
+  int n_max;
+  if (ele->key == BGO_QUADRUPOLE) n_max = 1;
+  else if (ele->key == BGO_SEXTUPOLE) n_max = 2;
+  else return;
+  double x = orb->vec[0], y = orb->vec[2];
+  bgo_cplx xy = {x, y}, poly_n1 = {1.0, 0.0}, poly = xy, poly_n2;
+  double rel_p = 1 + orb->vec[5];
+  double fx = 0, dfx_dx = 0, dfx_dy = 0, fy = 0, dfy_dx = 0, dfy_dy = 0;
+  FL(1);
+  for (int n = 1; n <= n_max; n++) {
+    poly_n2 = poly_n1;
+    poly_n1 = poly;
+    poly = cmul(poly, xy);
+    double ap = 0, bp;
+    if (ele->key == BGO_QUADRUPOLE) {
+      bp = ele->k1;
+    } else {
+      bp = ele->k2;
+      if (n != 2) continue;
+    }
+    (void)poly_n2;
+    bgo_cplx dpoly_dx = {(n + 1) * poly_n1.re, (n + 1) * poly_n1.im};
+    bgo_cplx dpoly_dy = {-dpoly_dx.im, dpoly_dx.re}; /* i * dpoly_dx */
+    double den = (4 * (n + 2)) * rel_p;
+    bgo_cplx cab = {1.0 * bp / den, 1.0 * ap / den};
+    if (first_edge) {
+      cab.re = -cab.re;
+      cab.im = -cab.im;
+    }
+    double cn = (double)(n + 3) / (n + 1);
+    bgo_cplx xny = {x, -cn * y};
+    bgo_cplx dxny_dy = {0.0, -cn};
+    FL(8);
+    fx = fx + cmul(cmul(cab, poly), xny).re;
+    dfx_dx = dfx_dx + cmul(cab, cadd(cmul(dpoly_dx, xny), poly)).re;
+    dfx_dy = dfx_dy + cmul(cab, cadd(cmul(dpoly_dy, xny), cmul(poly, dxny_dy))).re;
+    xny = (bgo_cplx){y, cn * x};
+    bgo_cplx dxny_dx = {0.0, cn};
+    fy = fy + cmul(cmul(cab, poly), xny).re;
+    dfy_dx = dfy_dx + cmul(cab, cadd(cmul(dpoly_dx, xny), cmul(poly, dxny_dx))).re;
+    dfy_dy = dfy_dy + cmul(cab, cadd(cmul(dpoly_dy, xny), poly)).re;
+    FL(7);
+  }
+  double px = orb->vec[1], py = orb->vec[3];
+  double denom = (1 - dfx_dx) * (1 - dfy_dy) - dfx_dy * dfy_dx;
+  orb->vec[0] = orb->vec[0] - fx;
+  orb->vec[1] = px + ((1.0 - dfy_dy - denom) * px + dfy_dx * py) / denom;
+  orb->vec[2] = orb->vec[2] - fy;
+  orb->vec[3] = py + (dfx_dy * px + (1.0 - dfx_dx - denom) * py) / denom;
+  orb->vec[4] = orb->vec[4] + (orb->vec[1] * fx + orb->vec[3] * fy) / rel_p;
+  FL(26);
+}
+
 /* apply_element_edge_kick, bmad/low_level/apply_element_edge_kick.f90:37-278
  * for the bmad_standard field_calc case.  Returns -1 for unsupported forms. */
 static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first_edge, const bgo_param* param,
@@ -1287,14 +1360,13 @@ static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first
   if (!first_edge) electric_longitudinal_fringe(orb, ele, ae, be, ix_elec_max, at_sign, param);
   switch (ele->key) {
     case BGO_QUADRUPOLE:
-      /* hard_multipole_edge_kick (full, hard_edge_only) and
-       * soft_quadrupole_edge_kick (full, soft_edge_only) are not restated */
-      if (ele->fringe_type == BGO_FRINGE_FULL || ele->fringe_type == BGO_FRINGE_SOFT_EDGE_ONLY ||
-          ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY)
-        return -1;
-      break;
     case BGO_SEXTUPOLE:
-      if (ele->fringe_type == BGO_FRINGE_FULL || ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY) return -1;
+      /* apply_element_edge_kick.f90:173-186: quadrupole entrance hard then
+       * soft, exit soft then hard; sextupole hard only.  The soft
+       * quadrupole edge (soft_quadrupole_edge_kick, fringe_mod.f90:555-660)
+       * is zero for fq1 = fq2 = 0, the defaults, which are assumed here. */
+      if (ele->fringe_type == BGO_FRINGE_FULL || ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY)
+        hard_multipole_edge_kick(ele, first_edge, orb);
       break;
     case BGO_SBEND:
       /* bend_edge_kick, fringe_mod.f90:39-127: fringe_here, hard multipole edge

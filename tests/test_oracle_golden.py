@@ -77,9 +77,14 @@ ELEMENTS = {
     "RFCAVITY3": ("rfcavity", {"rf_frequency": 500e6, "voltage": 1e5, "phi0": 0.1, "x_offset": 0.05,
                                "y_pitch": 0.001, "tilt": 0.1}, {"num_steps": 10, "a_pole": {2: 0.02}}),
 }
-for _n, _k1 in (("QUADRUPOLE1", 1.0), ("QUADRUPOLE2", -1.0), ("QUADRUPOLE3", 1e-20)):
+for _n, _k1, _fr in (("QUADRUPOLE1", 1.0, None), ("QUADRUPOLE2", -1.0, None), ("QUADRUPOLE3", 1e-20, None),
+                     ("QUADRUPOLE4", 1.0, "full"), ("QUADRUPOLE5", -1.0, "full")):
     _q = q0(l=0.6, k1=_k1, tilt=PI / 4, x_offset=0.05, y_pitch=0.001)
-    ELEMENTS[_n] = ("quadrupole", _q.pop("values"), dict(num_steps=10, **_q))
+    _kw = dict(num_steps=10, **_q)
+    _kw.pop("values")
+    if _fr:
+        _kw["fringe_type"] = _fr
+    ELEMENTS[_n] = ("quadrupole", _q["values"], _kw)
 
 
 def make_element(name):
