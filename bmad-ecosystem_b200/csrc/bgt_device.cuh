@@ -520,6 +520,54 @@ __device__ __forceinline__ void electric_longitudinal_fringe(Part& p, const doub
   apply_energy_kick(p, -ff * phi, G);
 }
 
+// hard_multipole_edge_kick, bmad/modules/fringe_mod.f90:691-864 (tracking
+// part): hard-edge fringe of the quadrupole (N = 1, bp = k1) or sextupole
+// (N = 2, bp = k2) body field, charge_dir = 1.  Complex products as gfortran
+// forms them: (a + ib)(c + id) = (ac - bd) + i(ad + bc).
+struct Cx {
+  double re, im;
+};
+__device__ __forceinline__ Cx cx_mul(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ Cx cx_add(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+
+template <int N>
+__device__ __forceinline__ void hard_multipole_edge_kick(Part& p, double bp, bool first_edge) {
+  const double x = p.x, y = p.y;
+  const Cx xy = {x, y};
+  Cx poly_n1 = {1.0, 0.0}, poly = xy;
+  const double rel_p = 1 + p.pz;
+  double fx = 0, dfx_dx = 0, dfx_dy = 0, fy = 0, dfy_dx = 0, dfy_dy = 0;
+#pragma unroll
+  for (int n = 1; n <= N; n++) {
+    poly_n1 = poly;
+    poly = cx_mul(poly, xy);
+    if (n != N) continue;  // a sextupole's field is order 2 only
+    const Cx dpoly_dx = {(n + 1) * poly_n1.re, (n + 1) * poly_n1.im};
+    const Cx dpoly_dy = {-dpoly_dx.im, dpoly_dx.re};
+    const double den = (4 * (n + 2)) * rel_p;
+    Cx cab = {1.0 * bp / den, 1.0 * 0.0 / den};
+    if (first_edge) cab = {-cab.re, -cab.im};
+    const double cn = (double)(n + 3) / (n + 1);
+    Cx xny = {x, -cn * y};
+    const Cx dxny_dy = {0.0, -cn};
+    fx = fx + cx_mul(cx_mul(cab, poly), xny).re;
+    dfx_dx = dfx_dx + cx_mul(cab, cx_add(cx_mul(dpoly_dx, xny), poly)).re;
+    dfx_dy = dfx_dy + cx_mul(cab, cx_add(cx_mul(dpoly_dy, xny), cx_mul(poly, dxny_dy))).re;
+    xny = {y, cn * x};
+    const Cx dxny_dx = {0.0, cn};
+    fy = fy + cx_mul(cx_mul(cab, poly), xny).re;
+    dfy_dx = dfy_dx + cx_mul(cab, cx_add(cx_mul(dpoly_dx, xny), cx_mul(poly, dxny_dx))).re;
+    dfy_dy = dfy_dy + cx_mul(cab, cx_add(cx_mul(dpoly_dy, xny), poly)).re;
+  }
+  const double px = p.px, py = p.py;
+  const double denom = (1 - dfx_dx) * (1 - dfy_dy) - dfx_dy * dfy_dx;
+  p.x = p.x - fx;
+  p.px = px + ((1.0 - dfy_dy - denom) * px + dfy_dx * py) / denom;
+  p.y = p.y - fy;
+  p.py = py + (dfx_dy * px + (1.0 - dfx_dx - denom) * py) / denom;
+  p.z = p.z + (p.px * fx + p.py * fy) / rel_p;
+}
+
 // ---------------------------------------------------------------------------
 // Hwang hard-edge bend fringe, bmad/modules/fringe_mod.f90:240-418 (td = +1)
 template <bool ENTERING>

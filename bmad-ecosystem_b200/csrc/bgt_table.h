@@ -46,9 +46,14 @@ enum Flag : int32_t {
   // electric multipoles): the state is checked after each edge kick
   F_FRINGE_INFO = 1 << 15,
   // quadrupole / thick multipole: electric multipoles, ae[aux1+1] and
-  // be[aux1+1] follow the magnetic an/bn arrays; F_EDGE_IN / F_EDGE_OUT then
-  // mark the ends with an electric longitudinal fringe kick
+  // be[aux1+1] follow the magnetic an/bn arrays.  For these kinds
+  // F_EDGE_IN / F_EDGE_OUT mark the ends fringe_at names
   F_ELEC = 1 << 16,
+  // the electric longitudinal fringe acts (electric multipoles, length != 0)
+  F_ELEC_EDGE = 1 << 17,
+  // quadrupole / sextupole hard-edge multipole fringe (fringe_type full or
+  // hard_edge_only); the body strength (k1 or k2) follows the arrays
+  F_HARD_EDGE = 1 << 18,
 };
 
 struct RecHdr {

@@ -81,9 +81,14 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
   const double* bn = an + (ix + 1);
   const double* ae = an + 2 * (ix + 1);
   const double* be = ae + (ixe + 1);
+  const double* hard = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
   if (fl & F_FRINGE_INFO) {
-    if (fl & F_EDGE_IN) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+    // apply_element_edge_kick.f90:160-176, first edge: magnetic, then electric
+    if (fl & F_EDGE_IN) {
+      if (fl & F_HARD_EDGE) hard_multipole_edge_kick<1>(p, hard[0], true);
+      if (fl & F_ELEC_EDGE) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+    }
     if (p.state != ALIVE) return;
   }
   if (ix > -1) ab_multipole_kicks(p, an, bn, ix, q[Q_RHALF]);
@@ -128,7 +133,11 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
     if (ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, (i == n_step) ? q[Q_STEP] / 2 : q[Q_STEP], G);
   }
   if (fl & F_FRINGE_INFO) {
-    if (fl & F_EDGE_OUT) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+    // second edge: electric, then magnetic
+    if (fl & F_EDGE_OUT) {
+      if (fl & F_ELEC_EDGE) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+      if (fl & F_HARD_EDGE) hard_multipole_edge_kick<1>(p, hard[0], false);
+    }
     if (p.state != ALIVE) return;
   }
   if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
@@ -145,9 +154,13 @@ __device__ __forceinline__ void body_thick(Part& p, const Rec& R, const Glob& G,
   const double* bn = an + (ix + 1);
   const double* ae = an + 2 * (ix + 1);
   const double* be = ae + (ixe + 1);
+  const double* hard = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
   if (fl & F_FRINGE_INFO) {
-    if (fl & F_EDGE_IN) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+    if (fl & F_EDGE_IN) {
+      if (fl & F_HARD_EDGE) hard_multipole_edge_kick<2>(p, hard[0], true);
+      if (fl & F_ELEC_EDGE) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+    }
     if (p.state != ALIVE) return;
   }
   if (ix > -1) ab_multipole_kicks(p, an, bn, ix, q[TM_RHALF]);
@@ -158,7 +171,10 @@ __device__ __forceinline__ void body_thick(Part& p, const Rec& R, const Glob& G,
     if (ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, (i == n_step) ? q[TM_STEP] / 2 : q[TM_STEP], G);
   }
   if (fl & F_FRINGE_INFO) {
-    if (fl & F_EDGE_OUT) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+    if (fl & F_EDGE_OUT) {
+      if (fl & F_ELEC_EDGE) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+      if (fl & F_HARD_EDGE) hard_multipole_edge_kick<2>(p, hard[0], false);
+    }
     if (p.state != ALIVE) return;
   }
   if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
@@ -1122,10 +1138,6 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       break;
     }
     case K_QUAD: {
-      if (e.fringe_type != BGT_FRINGE_NONE && e.fringe_at != BGT_NO_END) {
-        err = ename(e) + ": quadrupole fringe fields are not supported";
-        return BGT_EUNSUPPORTED;
-      }
       // pull_this_b1 (multipole_ele_to_ab.f90:660-676)
       double b1 = bn[1];
       bn[1] = 0;
@@ -1148,13 +1160,6 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       break;
     }
     case K_THICK_MULT: {
-      if (e.fringe_type == BGT_FRINGE_FULL || e.fringe_type == BGT_FRINGE_HARD_EDGE_ONLY ||
-          e.fringe_type == BGT_FRINGE_SOFT_EDGE_ONLY) {
-        if (key == BGT_SEXTUPOLE && e.fringe_at != BGT_NO_END && e.fringe_type != BGT_FRINGE_SOFT_EDGE_ONLY) {
-          err = ename(e) + ": sextupole hard-edge fringe is not supported";
-          return BGT_EUNSUPPORTED;
-        }
-      }
       if (key == BGT_PIPE) ix = -1;  // multipole_ele_to_ab returns nothing for pipes
       double length = e.l * 1;
       int n_step = (ix == -1 && ixe == -1) ? 1 : std::max(nint_h(fabs(length / e.ds_step)), 1);
@@ -1309,9 +1314,12 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
   }
   h.aux1 = -1;
   if (kind == K_QUAD || kind == K_THICK_MULT) {
-    // init_fringe_info (bmad/low_level/init_fringe_info.f90:22-60)
+    // init_fringe_info (bmad/low_level/init_fringe_info.f90:22-60); the edge
+    // kicks act at the ends fringe_at names (apply_element_edge_kick.f90:104)
     const bool fringe = (e.fringe_type != BGT_FRINGE_NONE && e.fringe_at != BGT_NO_END) || ixe > -1;
     if (fringe) flags |= F_FRINGE_INFO;
+    if (e.fringe_at == BGT_ENTRANCE_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_IN;
+    if (e.fringe_at == BGT_EXIT_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_OUT;
     if (ixe > -1) {
       flags |= F_ELEC;
       h.aux1 = ixe;
@@ -1321,11 +1329,17 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
         q[ixe + 1 + n] = e.bn_elec[n];
       }
       // electric_longitudinal_fringe (apply_element_edge_kick.f90:283-329)
-      // acts at the ends fringe_at names, and not at all for zero length
-      if (e.l != 0) {
-        if (e.fringe_at == BGT_ENTRANCE_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_IN;
-        if (e.fringe_at == BGT_EXIT_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_OUT;
-      }
+      // does nothing for zero length
+      if (e.l != 0) flags |= F_ELEC_EDGE;
+    }
+    // hard_multipole_edge_kick (fringe_mod.f90:691-864) for quadrupoles and
+    // sextupoles; soft_quadrupole_edge_kick is zero for fq1 = fq2 = 0 (the
+    // defaults, the only values this table carries)
+    if ((e.fringe_type == BGT_FRINGE_FULL || e.fringe_type == BGT_FRINGE_HARD_EDGE_ONLY) &&
+        (key == BGT_QUADRUPOLE || key == BGT_SEXTUPOLE)) {
+      flags |= F_HARD_EDGE;
+      double* q = B.ptr_after_push(1);
+      q[0] = (key == BGT_QUADRUPOLE) ? e.k1 : e.k2;
     }
   }
   h.flags = flags;
