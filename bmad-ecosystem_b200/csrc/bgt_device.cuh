@@ -119,10 +119,48 @@ __device__ __forceinline__ bool orbit_too_large(Part& p, const Glob& G) {
 
 // bmad/low_level/check_aperture_limit.f90:240-309 (lab-frame elliptical and
 // rectangular limits; the leading orbit_too_large is done by the caller).
-__device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32_t flags) {
+// (x, y) checked against the limits: x, y themselves, or with
+// offset_moves_aperture the particle's position in the element frame at this
+// end -- offset_particle(set, s_pos = 0 or L, no drift, tilt for collimators)
+// as check_aperture_limit.f90:159-175 calls it (only x and y are needed).
+__device__ __forceinline__ void aperture_frame(const Part& p, const double* mis, int32_t flags, bool at_exit,
+                                               double& xa, double& ya) {
+  xa = p.x;
+  ya = p.y;
+  if (!(flags & F_AP_OFFSET)) return;
+  if (flags & F_OFFSET) {
+    if (flags & F_PITCH) {
+      const double rel_p = 1 + p.pz;
+      const double r0 = p.x - mis[MIS_XOFF], r1 = p.y - mis[MIS_YOFF];
+      const double r2 = at_exit ? mis[MIS_R3EXIT] : mis[MIS_R3SET];
+      const double* w = mis + MIS_WINV;
+      const double o0 = w[0] * r0 + w[1] * r1 + w[2] * r2;
+      const double o1 = w[3] * r0 + w[4] * r1 + w[5] * r2;
+      const double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+      if (pz > 0) {  // with pz <= 0 offset_particle only marks the particle
+        xa = o0;
+        ya = o1;
+      }
+    } else {
+      const double rel_p = 1 + p.pz;
+      const double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+      if (pz > 0) {
+        xa = p.x - mis[MIS_XOFF];
+        ya = p.y - mis[MIS_YOFF];
+      }
+    }
+  }
+  if ((flags & F_AP_TILT) && (flags & F_TILT)) {
+    const double c = mis[MIS_COS], s = mis[MIS_SIN], x = xa, y = ya;
+    xa = c * x + s * y;
+    ya = -s * x + c * y;
+  }
+}
+
+__device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32_t flags, double px_, double py_) {
   if (flags & F_AP_ELLIPTICAL) {
-    double xp = p.x - ap[AP_XC];
-    double yp = p.y - ap[AP_YC];
+    double xp = px_ - ap[AP_XC];
+    double yp = py_ - ap[AP_YC];
     double r = sq(xp / ap[AP_XW]) + sq(yp / ap[AP_YW]);
     if (r < 1) return;
     if (fabs(xp / ap[AP_XW]) > fabs(yp / ap[AP_YW])) {
@@ -133,35 +171,43 @@ __device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32
   } else {
     double uf = 0, f;
     const double x1 = ap[AP_X1], x2 = ap[AP_X2], y1 = ap[AP_Y1], y2 = ap[AP_Y2];
-    if (x1 != 0 && p.x < x1) {
-      f = fabs((p.x - x1) / (x2 - x1));
+    const double xv = px_, yv = py_;
+    if (x1 != 0 && xv < x1) {
+      f = fabs((xv - x1) / (x2 - x1));
       if (f > uf) {
         p.state = LOST_NEG_X;
         uf = f;
       }
     }
-    if (x2 != 0 && p.x > x2) {
-      f = fabs((p.x - x2) / (x2 - x1));
+    if (x2 != 0 && xv > x2) {
+      f = fabs((xv - x2) / (x2 - x1));
       if (f > uf) {
         p.state = LOST_POS_X;
         uf = f;
       }
     }
-    if (y1 != 0 && p.y < y1) {
-      f = fabs((p.y - y1) / (y2 - y1));
+    if (y1 != 0 && yv < y1) {
+      f = fabs((yv - y1) / (y2 - y1));
       if (f > uf) {
         p.state = LOST_NEG_Y;
         uf = f;
       }
     }
-    if (y2 != 0 && p.y > y2) {
-      f = fabs((p.y - y2) / (y2 - y1));
+    if (y2 != 0 && yv > y2) {
+      f = fabs((yv - y2) / (y2 - y1));
       if (f > uf) {
         p.state = LOST_POS_Y;
         uf = f;
       }
     }
   }
+}
+
+__device__ __forceinline__ void check_aperture(Part& p, const double* ap, const double* mis, int32_t flags,
+                                               bool at_exit) {
+  double xa, ya;
+  aperture_frame(p, mis, flags, at_exit, xa, ya);
+  aperture_limits(p, ap, flags, xa, ya);
 }
 
 // ---------------------------------------------------------------------------

@@ -54,6 +54,11 @@ enum Flag : int32_t {
   // quadrupole / sextupole hard-edge multipole fringe (fringe_type full or
   // hard_edge_only); the body strength (k1 or k2) follows the arrays
   F_HARD_EDGE = 1 << 18,
+  // offset_moves_aperture: the aperture is checked in the element frame
+  // (check_aperture_limit.f90:159-175); F_AP_TILT: with the tilt as well
+  // (collimators)
+  F_AP_OFFSET = 1 << 19,
+  F_AP_TILT = 1 << 20,
 };
 
 struct RecHdr {
@@ -85,7 +90,8 @@ constexpr int MIS_R3SET = 28;     // 0 - (z_offset + ds_center) on set
 constexpr int MIS_R3UNSET = 29;   // 0 - ds_center on unset
 constexpr int MIS_ZADD = 30;      // z_offset + L/2 on unset
 constexpr int MIS_COSU = 31, MIS_SINU = 32;  // cos/sin of -tilt (unset)
-constexpr int MIS_N = 33;
+constexpr int MIS_R3EXIT = 33;    // 0 - (z_offset + ds_center) with s = L (aperture at the exit)
+constexpr int MIS_N = 34;
 
 constexpr int AP_X1 = 0, AP_X2 = 1, AP_Y1 = 2, AP_Y2 = 3;  // x1_lim = -x1_limit, ...
 constexpr int AP_XW = 4, AP_XC = 5, AP_YW = 6, AP_YC = 7;  // elliptical width2/center

@@ -503,7 +503,7 @@ __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glo
   Rec R = decode(rec);
   const int32_t fl = R.h->flags;
   if ((fl & F_AP_ENTRANCE) && G.ap_on) {
-    aperture_limits(p, R.ap, fl);
+    check_aperture(p, R.ap, R.mis, fl, false);
     if (p.state != ALIVE) return;
   }
   switch (R.h->kind) {
@@ -530,7 +530,7 @@ __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glo
   }
   if (orbit_too_large(p, G)) return;
   if (p.state != ALIVE) return;
-  if ((fl & F_AP_EXIT) && G.ap_on) aperture_limits(p, R.ap, fl);
+  if ((fl & F_AP_EXIT) && G.ap_on) check_aperture(p, R.ap, R.mis, fl, true);
 }
 
 // ===========================================================================
@@ -1064,9 +1064,13 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     }
   }
   if (ap_any) {
-    if (e.offset_moves_aperture && (offset || tilt != 0)) {
-      err = ename(e) + ": offset_moves_aperture with a misaligned element is not supported";
-      return BGT_EUNSUPPORTED;
+    if (e.offset_moves_aperture && (flags & F_MISALIGN) && (offset || tilt != 0)) {
+      if (kind == K_BEND) {
+        err = ename(e) + ": offset_moves_aperture on a bend is not supported";
+        return BGT_EUNSUPPORTED;
+      }
+      flags |= F_AP_OFFSET;
+      if (key == BGT_ECOLLIMATOR || key == BGT_RCOLLIMATOR) flags |= F_AP_TILT;
     }
     if (e.aperture_at == BGT_ENTRANCE_END || e.aperture_at == BGT_BOTH_ENDS) flags |= F_AP_ENTRANCE;
     if (e.aperture_at == BGT_EXIT_END || e.aperture_at == BGT_BOTH_ENDS) flags |= F_AP_EXIT;
@@ -1097,6 +1101,9 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     double ds_center_unset = L_half - L;
     m[MIS_R3UNSET] = 0.0 - ds_center_unset;
     m[MIS_ZADD] = e.z_offset + L_half;
+    // aperture in the element frame at the exit: s_pos = L
+    double ds_center_exit = L_half - L;
+    m[MIS_R3EXIT] = 0.0 - (e.z_offset + 1 * ds_center_exit);
     double s_lab = m[MIS_R3UNSET] + m[MIS_ZADD];
     m[MIS_DS_UNSET] = (1 + 1) * L_half - s_lab;
   }
