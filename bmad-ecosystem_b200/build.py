@@ -16,6 +16,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 SRCS = [HERE / "csrc" / "bgt_track.cu", HERE / "csrc" / "bgt_mlp.cu"]
+# the tracking kernel's instances, one compilation per group (bgt_track_kernels.cu)
+KERNEL_SRC = HERE / "csrc" / "bgt_track_kernels.cu"
+N_KERNEL_GROUPS = 10
 OUT = HERE / "bgt" / "libbgt.so"
 
 
@@ -37,9 +40,12 @@ def build(fmad: bool = False, out: Path = OUT, verbose: bool = False) -> Path:
         common.insert(1, "-Xptxas=-v")
     objdir = out.parent / "_obj"
     objdir.mkdir(exist_ok=True)
-    objs = [objdir / (s.stem + ".o") for s in SRCS]
-    procs = [subprocess.Popen(common + ["-c", "-o", str(o), str(s)], stdout=subprocess.PIPE, stderr=subprocess.PIPE,
-                              text=True) for s, o in zip(SRCS, objs)]
+    jobs = [([], s, objdir / (s.stem + ".o")) for s in SRCS]
+    jobs += [([f"-DBGT_KERNEL_GROUP={g}"], KERNEL_SRC, objdir / f"{KERNEL_SRC.stem}_{g}.o")
+             for g in range(N_KERNEL_GROUPS)]
+    objs = [o for _, _, o in jobs]
+    procs = [subprocess.Popen(common + d + ["-c", "-o", str(o), str(s)], stdout=subprocess.PIPE,
+                              stderr=subprocess.PIPE, text=True) for d, s, o in jobs]
     errs = []
     for p in procs:
         so, se = p.communicate()

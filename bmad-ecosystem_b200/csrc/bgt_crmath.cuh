@@ -27,7 +27,7 @@
 #ifdef __CUDACC__
 #define BGT_HD __host__ __device__ __forceinline__
 // accurate paths run rarely: kept out of line so the hot loop stays small
-#define BGT_HD_NOINLINE __host__ __device__ __noinline__
+#define BGT_HD_NOINLINE static __host__ __device__ __noinline__
 #else
 #define BGT_HD static inline
 #define BGT_HD_NOINLINE static __attribute__((noinline))

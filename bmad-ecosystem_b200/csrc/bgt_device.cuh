@@ -76,10 +76,12 @@ __device__ __forceinline__ double powi_d(double x, int m) {
 __device__ __forceinline__ double mexp_d(double x, int m) { return m == 0 ? 1.0 : powi_d(x, m); }
 
 // c_multi(n, m, .true.) table (bmad/low_level/c_multi.f90:19-75), host-built.
-__constant__ double c_cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
+// Internal linkage: every compilation unit holding tracking kernels has its
+// own copy, filled through that unit's upload function.
+static __constant__ double c_cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
 // c_multi(n, m) without the n! factor (the cc table of multipole_kick,
 // multipole_mod.f90:262-266).
-__constant__ double c_cm0[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
+static __constant__ double c_cm0[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
 
 // ---------------------------------------------------------------------------
 // Apertures
