@@ -64,6 +64,42 @@ _VALUE_NAMES = [
 ]
 
 
+def rbend_to_sbend(values: Dict[str, float]) -> Dict[str, float]:
+    """An rbend given by its chord length ``l`` and ``g`` or ``angle`` as the
+    sbend the parser makes of it (bmad/parsing/bmad_parser_mod.f90:5080-5198,
+    fiducial_pt = none): the arc length, the bend angle, the edge angles each
+    increased by half the bend angle, and g = angle / l."""
+    v = dict(values)
+    l_chord = float(v.pop("l", 0.0))
+    angle = float(v.pop("angle", 0.0))
+    g = float(v.get("g", 0.0))
+    if g != 0 and angle != 0:
+        raise ValueError("rbend: give g or angle, not both")
+    length = 0.0
+    if l_chord != 0:
+        if angle != 0:
+            length = l_chord * angle / (2.0 * math.sin(0.5 * angle))
+        elif g != 0:
+            a = 0.5 * l_chord * g
+            if abs(a) >= 1:
+                raise ValueError("rbend: g * l is too large to be physical")
+            a = 2.0 * math.asin(a)
+            length = l_chord * a / (2.0 * math.sin(0.5 * a))
+        else:
+            length = l_chord
+    if length != 0 and angle != 0:
+        g = angle / length
+    elif g != 0:
+        angle = g * length
+    v["e1"] = float(v.get("e1", 0.0)) + 0.5 * angle
+    v["e2"] = float(v.get("e2", 0.0)) + 0.5 * angle
+    if angle != 0:
+        g = angle / length
+    v["g"] = g
+    v["l"] = length
+    return v
+
+
 @dataclass
 class Element:
     """One Bmad lattice element (a subset of ``ele_struct``)."""
@@ -95,6 +131,9 @@ class Element:
     user_ds_step: Optional[float] = None
 
     def __post_init__(self):
+        if self.key == "rbend":
+            self.values = rbend_to_sbend(self.values)
+            self.key = "sbend"
         if self.key not in KEYS:
             raise ValueError(f"unsupported element key {self.key!r}")
         if self.fringe_type is None:

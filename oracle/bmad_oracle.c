@@ -878,8 +878,184 @@ static void matvec3(double w[3][3], const double r[3], double out[3]) {
   }
 }
 
-/* offset_particle, bmad/code/offset_particle.f90:66-530 -- non-bend
- * geometry (bends support only the ref_tilt rotation), forward tracking.
+/* ------------------------------------------------------------------ */
+/* Bend geometry of offset_particle (offset_particle.f90:208-235 set,
+ * :393-425 unset).  Element constants (angles, tilts) use the C library. */
+
+enum { AX_X = 0, AX_Y = 1, AX_Z = 2 };
+
+typedef struct {
+  double r[3];
+  double w[3][3];
+} bgo_pos;
+
+/* sim_utils/special_functions/cos_one.f90:16-26 */
+static double cos_one(double angle) {
+  double s = sin(angle / 2);
+  return -(2 * (s * s));
+}
+
+/* rotate_vec, sim_utils/math/rotation_3d_mod.f90:737-760 */
+static void rotate_vec(double v[3], int axis, double angle) {
+  if (angle == 0) return;
+  double ca = cos(angle), sa = sin(angle), a, b;
+  if (axis == AX_X) {
+    a = ca * v[1] - sa * v[2];
+    b = sa * v[1] + ca * v[2];
+    v[1] = a;
+    v[2] = b;
+  } else if (axis == AX_Y) {
+    a = sa * v[2] + ca * v[0];
+    b = ca * v[2] - sa * v[0];
+    v[0] = a;
+    v[2] = b;
+  } else {
+    a = ca * v[0] - sa * v[1];
+    b = sa * v[0] + ca * v[1];
+    v[0] = a;
+    v[1] = b;
+  }
+}
+
+/* rotate_mat without right_multiply (mat = Rot . mat),
+ * sim_utils/math/rotation_3d_mod.f90:781-835: each column as rotate_vec */
+static void rotate_mat(double m[3][3], int axis, double angle) {
+  if (angle == 0) return;
+  for (int j = 0; j < 3; j++) {
+    double v[3] = {m[0][j], m[1][j], m[2][j]};
+    rotate_vec(v, axis, angle);
+    m[0][j] = v[0];
+    m[1][j] = v[1];
+    m[2][j] = v[2];
+  }
+}
+
+/* matmul of 3x3 matrices (k-ordered sums, as gfortran's inline matmul) */
+static void matmul33(double a[3][3], double b[3][3], double out[3][3]) {
+  double t[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0;
+      for (int k = 0; k < 3; k++) s = s + a[i][k] * b[k][j];
+      t[i][j] = s;
+    }
+  memcpy(out, t, sizeof(t));
+}
+
+/* w_mat_for_tilt, bmad/geometry/w_mat_for_tilt.f90:13-40 (not inverse) */
+static void w_mat_for_tilt(double tilt, double w[3][3]) {
+  double c = cos(tilt), s = sin(tilt);
+  double t[3][3] = {{c, -s, 0.0}, {s, c, 0.0}, {0.0, 0.0, 1.0}};
+  memcpy(w, t, sizeof(t));
+}
+
+static void pos_apply(bgo_pos* p, double m[3][3]) {
+  double r[3];
+  matvec3(m, p->r, r);
+  memcpy(p->r, r, sizeof(r));
+  matmul33(m, p->w, p->w);
+}
+
+/* bend_shift, bmad/geometry/bend_shift.f90:19-61; has_tilt says whether
+ * the optional ref_tilt argument is present. */
+static void bend_shift(bgo_pos* p, double g, double delta_s, int has_tilt, double ref_tilt) {
+  double angle = delta_s * g;
+  if (angle == 0) {
+    p->r[2] = p->r[2] - delta_s;
+    return;
+  }
+  double tlt = has_tilt ? ref_tilt : 0.0;
+  double S[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  if (tlt != 0) {
+    rotate_mat(S, AX_Z, -ref_tilt);
+    rotate_mat(S, AX_Y, angle);
+    rotate_mat(S, AX_Z, ref_tilt);
+  } else {
+    rotate_mat(S, AX_Y, angle);
+  }
+  double L[3] = {cos_one(angle) / g, 0.0 / g, -sin(angle) / g};
+  if (has_tilt) rotate_vec(L, AX_Z, ref_tilt);
+  double r[3];
+  matvec3(S, p->r, r);
+  for (int i = 0; i < 3; i++) p->r[i] = r[i] + L[i];
+  matmul33(S, p->w, p->w);
+}
+
+/* ele_misalignment_L_S_calc, bmad/geometry/ele_misalignment_L_S_calc.f90:
+ * 16-50, sbend branch (angle = g L, rho = 1/g as the bookkeeper sets them) */
+static void bend_misalignment_L_S(const bgo_ele* ele, double L_mis[3], double S[3][3]) {
+  L_mis[0] = ele->x_offset;
+  L_mis[1] = ele->y_offset;
+  L_mis[2] = ele->z_offset;
+  if (ele->roll != 0) {
+    double angle = ele->g * ele->l;
+    double rho = ele->g == 0 ? 0.0 : 1 / ele->g;
+    double Lc[3] = {rho * cos_one(angle / 2), rho * 0.0, rho * sin(angle / 2)};
+    rotate_vec(Lc, AX_Y, angle / 2);
+    rotate_vec(Lc, AX_Z, ele->ref_tilt);
+    for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] - Lc[i];
+    rotate_vec(Lc, AX_Z, ele->roll);
+    for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] + Lc[i];
+  }
+  floor_angles_to_w_mat(ele->x_pitch, ele->y_pitch, ele->roll, S, 0);
+}
+
+/* The bend branch of offset_particle for a misaligned bend with g, ref_tilt
+ * or roll nonzero: (x, y) -> position (r, w) in the body frame (set) or the
+ * lab frame (unset).  drift_to = 0: s_pos given, no drift (rho*atan2 form). */
+static void bend_offset_position(const bgo_ele* ele, int set, int drift_to, double ds_center, double L_half,
+                                 double x, double y, bgo_pos* pos) {
+  const double g = ele->g, ref_tilt = ele->ref_tilt;
+  double L_mis[3], ws[3][3], wt[3][3];
+  pos->r[0] = x;
+  pos->r[1] = y;
+  pos->r[2] = 0.0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) pos->w[i][j] = (i == j) ? 1.0 : 0.0;
+  if (set) {
+    bend_shift(pos, g, 1 * ds_center, 1, ref_tilt);
+    bend_misalignment_L_S(ele, L_mis, ws);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
+    for (int i = 0; i < 3; i++) pos->r[i] = pos->r[i] - L_mis[i];
+    pos_apply(pos, wt);
+    if (ref_tilt != 0) {
+      bend_shift(pos, g, -L_half, 1, ref_tilt);
+      w_mat_for_tilt(-ref_tilt, ws);
+      pos_apply(pos, ws);
+      bend_shift(pos, g, L_half, 0, 0.0);
+    }
+    if (drift_to != 0) {
+      bend_shift(pos, g, -1 * 1 * L_half, 0, 0.0);
+      pos->r[2] = pos->r[2] + (1 - 1 * 1) * L_half;
+    } else {
+      double ds = (g == 0) ? -1 * ds_center : (1 / g) * P_ATAN2(pos->r[2] * g, 1.0 + pos->r[0] * g);
+      bend_shift(pos, g, ds, 0, 0.0);
+      pos->r[2] = pos->r[2] + L_half + ds;
+    }
+  } else {
+    bend_shift(pos, g, ds_center, 0, 0.0);
+    if (ref_tilt != 0) {
+      bend_shift(pos, g, -L_half, 0, 0.0);
+      w_mat_for_tilt(ref_tilt, ws);
+      pos_apply(pos, ws);
+      bend_shift(pos, g, L_half, 1, ref_tilt);
+    }
+    bend_misalignment_L_S(ele, L_mis, ws);
+    pos_apply(pos, ws);
+    for (int i = 0; i < 3; i++) pos->r[i] = pos->r[i] + L_mis[i];
+    if (drift_to != 0) {
+      bend_shift(pos, g, 1 * 1 * L_half, 1, ref_tilt);
+      pos->r[2] = pos->r[2] + (1 + 1 * 1) * L_half;
+    } else {
+      double ds = (g == 0) ? -ds_center : (1 / g) * P_ATAN2(pos->r[2] * g, 1.0 + pos->r[0] * g);
+      bend_shift(pos, g, ds, 1, ref_tilt);
+      pos->r[2] = pos->r[2] + L_half + ds;
+    }
+  }
+}
+
+/* offset_particle, bmad/code/offset_particle.f90:66-530, forward tracking.
  * s_pos_mode: 0 = normal (drift to the edge), 1 = s_pos given (no drift),
  * with s_pos the lab (set) / body (unset) position. */
 static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int set_tilt, int set_hvkicks,
@@ -914,13 +1090,19 @@ static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int s
   if (set) {
     double s_body;
     if (is_misaligned) {
-      /* bend geometry with misalignments is not restated (rejected at setup) */
-      r[0] = orbit->vec[0] - ele->x_offset;
-      r[1] = orbit->vec[2] - ele->y_offset;
-      r[2] = 0.0 - (ele->z_offset + 1 * ds_center);
-      floor_angles_to_w_mat(ele->x_pitch, ele->y_pitch, 0.0, w, 1);
-      matvec3(w, r, r2);
-      r2[2] = r2[2] + L_half;
+      if (key == BGO_SBEND && (ele->g != 0 || ele->ref_tilt != 0 || ele->roll != 0)) {
+        bgo_pos pos;
+        bend_offset_position(ele, 1, drift_to, ds_center, L_half, orbit->vec[0], orbit->vec[2], &pos);
+        memcpy(r2, pos.r, sizeof(r2));
+        memcpy(w, pos.w, sizeof(w));
+      } else {
+        r[0] = orbit->vec[0] - ele->x_offset;
+        r[1] = orbit->vec[2] - ele->y_offset;
+        r[2] = 0.0 - (ele->z_offset + 1 * ds_center);
+        floor_angles_to_w_mat(ele->x_pitch, ele->y_pitch, 0.0, w, 1);
+        matvec3(w, r, r2);
+        r2[2] = r2[2] + L_half;
+      }
       s_body = r2[2];
       double pz = rel_p * rel_p - orbit->vec[1] * orbit->vec[1] - orbit->vec[3] * orbit->vec[3];
       if (pz <= 0) {
@@ -972,15 +1154,22 @@ static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int s
     }
     double s_lab;
     if (is_misaligned) {
-      r[0] = orbit->vec[0];
-      r[1] = orbit->vec[2];
-      r[2] = 0.0;
-      r[2] = r[2] - ds_center;
-      floor_angles_to_w_mat(ele->x_pitch, ele->y_pitch, 0.0, w, 0);
-      matvec3(w, r, r2);
-      r2[0] = r2[0] + ele->x_offset;
-      r2[1] = r2[1] + ele->y_offset;
-      r2[2] = r2[2] + (ele->z_offset + L_half);
+      if (key == BGO_SBEND && (ele->g != 0 || ele->ref_tilt != 0 || ele->roll != 0)) {
+        bgo_pos pos;
+        bend_offset_position(ele, 0, drift_to, ds_center, L_half, orbit->vec[0], orbit->vec[2], &pos);
+        memcpy(r2, pos.r, sizeof(r2));
+        memcpy(w, pos.w, sizeof(w));
+      } else {
+        r[0] = orbit->vec[0];
+        r[1] = orbit->vec[2];
+        r[2] = 0.0;
+        r[2] = r[2] - ds_center;
+        floor_angles_to_w_mat(ele->x_pitch, ele->y_pitch, 0.0, w, 0);
+        matvec3(w, r, r2);
+        r2[0] = r2[0] + ele->x_offset;
+        r2[1] = r2[1] + ele->y_offset;
+        r2[2] = r2[2] + (ele->z_offset + L_half);
+      }
       s_lab = r2[2];
       double pz = rel_p * rel_p - orbit->vec[1] * orbit->vec[1] - orbit->vec[3] * orbit->vec[3];
       if (pz <= 0) {
@@ -1613,12 +1802,33 @@ static void sbend_body_with_k1_map(const bgo_ele* ele, double dg, double b1, int
   FL(110);
 }
 
+/* elec_multipole_field, bmad/code/elec_multipole_field.f90:20-65 (no dE) */
+static void elec_multipole_field(double a, double b, int n, const bgo_coord* coord, double* Ex, double* Ey) {
+  *Ex = 0;
+  *Ey = 0;
+  if (a == 0 && b == 0) return;
+  double x = coord->vec[0], y = coord->vec[2];
+  for (int m = 0; m <= n; m += 2) {
+    double f = bgo_c_multi(n, m, 1) * mexp(x, n - m) * mexp(y, m);
+    *Ex = *Ex - b * f;
+    *Ey = *Ey - a * f;
+  }
+  for (int m = 1; m <= n; m += 2) {
+    double f = bgo_c_multi(n, m, 1) * mexp(x, n - m) * mexp(y, m);
+    *Ex = *Ex + a * f;
+    *Ey = *Ey - b * f;
+  }
+}
+
 /* apply_multipole_kicks (contained in track_a_bend), track_a_bend.f90:338-471,
- * non-exact magnetic form.  Electric bend multipoles are not restated. */
-static void bend_apply_multipole_kicks(double coef, double r_step, int ix_mag_max, const double* an,
-                                       const double* bn, const bgo_ele* ele, bgo_coord* orbit,
+ * non-exact form: the magnetic field B and electric field E at the particle,
+ * then the magnetic kick, then the electric kick (which changes pz, beta, z). */
+static void bend_apply_multipole_kicks(double coef, double step_len, double r_step, int ix_mag_max,
+                                       const double* an, const double* bn, int ix_elec_max, const double* ae,
+                                       const double* be, const bgo_ele* ele, bgo_coord* orbit,
                                        const bgo_param* param) {
-  double B0 = 0, B1 = 0, kx, ky;
+  double B0 = 0, B1 = 0, E0 = 0, E1 = 0, kx, ky;
+  int charge = param->charge;
   double c_dir = 1 * 1 * (double)param->charge;
   double f_p0c = r_step * ele->p0c / (C_LIGHT * param->charge);
   for (int i = 0; i <= ix_mag_max; i++) {
@@ -1628,25 +1838,44 @@ static void bend_apply_multipole_kicks(double coef, double r_step, int ix_mag_ma
     B1 = B1 - f_p0c * kx;
     FL(4);
   }
+  for (int i = 0; i <= ix_elec_max; i++) {
+    if (ae[i] == 0 && be[i] == 0) continue;
+    double Ex, Ey;
+    elec_multipole_field(ae[i], be[i], i, orbit, &Ex, &Ey);
+    E0 = E0 + Ex;
+    E1 = E1 + Ey;
+  }
   if (ix_mag_max > -1) {
     double f_coef = coef * c_dir * (1 + ele->g * orbit->vec[0]) * C_LIGHT / orbit->p0c;
     orbit->vec[1] = orbit->vec[1] - f_coef * B1;
     orbit->vec[3] = orbit->vec[3] + f_coef * B0;
     FL(10);
   }
+  if (ix_elec_max > -1) {
+    bgo_coord orb0 = *orbit;
+    double rel_p0 = 1 + orb0.vec[5];
+    double ps2 = rel_p0 * rel_p0 - orb0.vec[1] * orb0.vec[1] - orb0.vec[3] * orb0.vec[3];
+    double ps = sqrt(ps2) / rel_p0;
+    double f_coef =
+        step_len * coef * (1 + ele->g * orb0.vec[0]) * (double)charge / (ps * orb0.beta * orb0.p0c);
+    double Kx = f_coef * E0;
+    double Ky = f_coef * E1;
+    double alpha = (Kx * (2 * orb0.vec[1] + Kx) + Ky * (2 * orb0.vec[3] + Ky)) / (rel_p0 * rel_p0);
+    orbit->vec[1] = orb0.vec[1] + Kx;
+    orbit->vec[3] = orb0.vec[3] + Ky;
+    orbit->vec[5] = orb0.vec[5] + rel_p0 * sqrt_one(alpha);
+    orbit->beta = (1 + orbit->vec[5]) / sqrt(ps2 + orbit->vec[1] * orbit->vec[1] + orbit->vec[3] * orbit->vec[3] +
+                                             sq(param->mass / orbit->p0c));
+    orbit->vec[4] = orb0.vec[4] * orbit->beta / orb0.beta;
+  }
 }
 
 /* track_a_bend, bmad/low_level/track_a_bend.f90:18-333 */
 static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) {
   double an[BGO_N_POLE], bn[BGO_N_POLE], ae[BGO_N_POLE], be[BGO_N_POLE], b1;
-  int is_misaligned = (ele->x_offset != 0 || ele->y_offset != 0 || ele->z_offset != 0 || ele->x_pitch != 0 ||
-                       ele->y_pitch != 0 || ele->roll != 0);
-  if (is_misaligned) return -1; /* bend misalignment geometry not restated */
-
   if (ele->has_misalign) offset_particle(ele, 1, orbit, 1, 0, 0, 0, param);
   double rel_charge_dir = 1.0;
   int ix_elec_max = bgo_multipole_ele_to_ab(ele, 0, 1, 0, ae, be, NULL);
-  if (ix_elec_max > -1) return -1; /* electric bend multipoles not restated */
   if (apply_element_edge_kick(orbit, ele, 1, param, ae, be, ix_elec_max)) return -1;
   if (bgo_orbit_too_large(orbit, param)) return 0;
 
@@ -1680,7 +1909,8 @@ static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) 
   double step_len = length / n_step;
   double angle = g * step_len;
   FL(4);
-  if (ix_mag_max > -1) bend_apply_multipole_kicks(0.5, r_step, ix_mag_max, an, bn, ele, orbit, param);
+  if (ix_mag_max > -1 || ix_elec_max > -1)
+    bend_apply_multipole_kicks(0.5, step_len, r_step, ix_mag_max, an, bn, ix_elec_max, ae, be, ele, orbit, param);
 
   for (int n = 1; n <= n_step; n++) {
     if (b1 != 0) {
@@ -1754,9 +1984,13 @@ static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) 
         FL(28);
       }
     }
-    if (ix_mag_max > -1) {
-      if (n == n_step) bend_apply_multipole_kicks(0.5, r_step, ix_mag_max, an, bn, ele, orbit, param);
-      else bend_apply_multipole_kicks(1.0, r_step, ix_mag_max, an, bn, ele, orbit, param);
+    if (ix_mag_max > -1 || ix_elec_max > -1) {
+      if (n == n_step)
+        bend_apply_multipole_kicks(0.5, step_len, r_step, ix_mag_max, an, bn, ix_elec_max, ae, be, ele, orbit,
+                                   param);
+      else
+        bend_apply_multipole_kicks(1.0, step_len, r_step, ix_mag_max, an, bn, ix_elec_max, ae, be, ele, orbit,
+                                   param);
     }
   }
   if (bgo_orbit_too_large(orbit, param)) return 0;

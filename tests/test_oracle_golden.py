@@ -48,6 +48,14 @@ def q0(**kw):
     return dict(values=vals, a_pole={0: 0.01, 1: 0.1}, a_pole_elec={1: 2e4}, b_pole_elec={0: -2e3})
 
 
+def sb0(**kw):
+    # sb0 / rb0: bend, a0 = 0.01, a1 = 0.1, vkick = -0.0001, b0_elec = -2e3,
+    # a1_elec = 2e4, r0_mag = 2, r0_elec = 3 (tracking_method_test.bmad:79-80)
+    vals = {"vkick": -0.0001, "r0_mag": 2.0, "r0_elec": 3.0}
+    vals.update(kw)
+    return dict(values=vals, a_pole={0: 0.01, 1: 0.1}, a_pole_elec={1: 2e4}, b_pole_elec={0: -2e3})
+
+
 # name -> (key, values, extra Element kwargs)
 ELEMENTS = {
     "DRIFT1": ("drift", {"l": 4.5, "x_offset": 0.05, "y_pitch": 0.001, "tilt": 0.1}, {"num_steps": 10}),
@@ -77,6 +85,15 @@ ELEMENTS = {
     "RFCAVITY3": ("rfcavity", {"rf_frequency": 500e6, "voltage": 1e5, "phi0": 0.1, "x_offset": 0.05,
                                "y_pitch": 0.001, "tilt": 0.1}, {"num_steps": 10, "a_pole": {2: 0.02}}),
 }
+# tracking_method_test.bmad:84,89-91 (the rows without exact multipoles or a
+# full bend fringe): misaligned bends with ref_tilt, electric multipoles
+for _n, _key, _b in (("SBEND3", "sbend", sb0(l=0.6, k1=0.3, k2=3.0, x_offset=0.05, y_pitch=0.001, ref_tilt=0.1)),
+                     ("RBEND6", "rbend", sb0(l=0.6, g=0.01, dg=-0.0099999, e1=0.1, e2=0.2, x_offset=0.05,
+                                             y_pitch=0.001, ref_tilt=0.1)),
+                     ("SBEND7", "sbend", sb0(l=0.6, g=0.01, e1=0.1, e2=0.2, x_offset=0.05, y_pitch=0.001,
+                                             ref_tilt=0.1))):
+    _kw = dict(num_steps=10, **_b)
+    ELEMENTS[_n] = (_key, _kw.pop("values"), _kw)
 for _n, _k1, _fr in (("QUADRUPOLE1", 1.0, None), ("QUADRUPOLE2", -1.0, None), ("QUADRUPOLE3", 1e-20, None),
                      ("QUADRUPOLE4", 1.0, "full"), ("QUADRUPOLE5", -1.0, "full")):
     _q = q0(l=0.6, k1=_k1, tilt=PI / 4, x_offset=0.05, y_pitch=0.001)
