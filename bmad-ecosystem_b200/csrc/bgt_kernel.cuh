@@ -34,6 +34,7 @@ struct Rec {
   const double* kb;    // kind block
 };
 
+template <bool RARE>
 __device__ __forceinline__ Rec decode(const double* r) {
   Rec R;
   R.h = reinterpret_cast<const RecHdr*>(r);
@@ -44,6 +45,7 @@ __device__ __forceinline__ Rec decode(const double* r) {
   if (fl & F_MISALIGN) {
     R.mis = q;
     q += MIS_N;
+    if (RARE && (fl & F_BEND_MIS)) q += BM_N;  // the bend geometry follows the block
   }
   if (fl & (F_AP_ENTRANCE | F_AP_EXIT)) {
     R.ap = q;
@@ -353,6 +355,107 @@ __device__ __forceinline__ void bend_multipole_kicks(Part& p, const double* q, c
   p.py = p.py + f_coef * B0;
 }
 
+// apply_multipole_kicks, electric part (track_a_bend.f90:379-385 field,
+// :421-438 kick): the field of elec_multipole_field (bmad/code/
+// elec_multipole_field.f90:20-65) summed over the orders, then the kick that
+// changes px, py, pz, beta and z.  Called after the magnetic kick, which does
+// not move x and y, so the field is the one the reference evaluates first.
+__device__ __forceinline__ void bend_elec_kicks(Part& p, const double* ae, const double* be, int ixe, double coef,
+                                                double step_len, double g, const Glob& G) {
+  double E0 = 0, E1 = 0;
+  const double x = p.x, y = p.y;
+  for (int n = 0; n <= ixe; n++) {
+    const double a = ae[n], b = be[n];
+    if (a == 0 && b == 0) continue;
+    double Ex = 0, Ey = 0;
+    for (int mm = 0; mm <= n; mm += 2) {
+      const double f = c_cm[n][mm] * mexp_d(x, n - mm) * mexp_d(y, mm);
+      Ex = Ex - b * f;
+      Ey = Ey - a * f;
+    }
+    for (int mm = 1; mm <= n; mm += 2) {
+      const double f = c_cm[n][mm] * mexp_d(x, n - mm) * mexp_d(y, mm);
+      Ex = Ex + a * f;
+      Ey = Ey - b * f;
+    }
+    E0 = E0 + Ex;
+    E1 = E1 + Ey;
+  }
+  const double px0 = p.px, py0 = p.py, pz0 = p.pz, z0 = p.z, beta0 = p.beta;
+  const double rel_p0 = 1 + pz0;
+  const double ps2 = rel_p0 * rel_p0 - px0 * px0 - py0 * py0;
+  const double ps = sqrt(ps2) / rel_p0;
+  const double f_coef = step_len * coef * (1 + g * x) * (double)G.charge / (ps * beta0 * G.p0c);
+  const double Kx = f_coef * E0;
+  const double Ky = f_coef * E1;
+  const double alpha = (Kx * (2 * px0 + Kx) + Ky * (2 * py0 + Ky)) / (rel_p0 * rel_p0);
+  p.px = px0 + Kx;
+  p.py = py0 + Ky;
+  p.pz = pz0 + rel_p0 * sqrt_one(alpha);
+  p.beta = (1 + p.pz) / sqrt(ps2 + p.px * p.px + p.py * p.py + sq(G.mc2 / G.p0c));
+  p.z = z0 * p.beta / beta0;
+}
+
+// 3x3 matrix times vector, sums from zero in k order (as the oracle's and
+// gfortran's matmul)
+__device__ __forceinline__ void mv3_0(const double* S, double r0, double r1, double r2, double& o0, double& o1,
+                                      double& o2) {
+  o0 = ((0.0 + S[0] * r0) + S[1] * r1) + S[2] * r2;
+  o1 = ((0.0 + S[3] * r0) + S[4] * r1) + S[5] * r2;
+  o2 = ((0.0 + S[6] * r0) + S[7] * r1) + S[8] * r2;
+}
+
+// offset_particle for a misaligned bend (offset_particle.f90:208-235 set,
+// :393-425 unset, drift to the edge): (x, y, 0) through the BM block's
+// affine steps, the momentum through their product W, then the drift to the
+// nominal edge (s = 0 on set, L on unset).
+__device__ __forceinline__ void bend_offset(Part& p, const double* bm, bool set, double L_half, const Glob& G,
+                                            DriftMemo& m) {
+  const int n = (int)bm[set ? BM_NSET : BM_NUNSET];
+  const double* ops = bm + (set ? BM_OPS_SET : BM_OPS_UNSET);
+  const double* W = bm + (set ? BM_WSET : BM_WUNSET);
+  double r0 = p.x, r1 = p.y, r2 = 0.0;
+  for (int k = 0; k < n; k++) {
+    const double* o = ops + k * BM_OP_N;
+    const int code = (int)o[0];
+    const double* S = o + 1;
+    const double* L = o + 10;
+    if (code == 0) {
+      r2 = r2 - L[2];
+    } else if (code == 4) {
+      r2 = r2 + L[2];
+    } else {
+      double a0 = r0, a1 = r1, a2 = r2;
+      if (code == 2) {
+        a0 = r0 - L[0];
+        a1 = r1 - L[1];
+        a2 = r2 - L[2];
+      }
+      mv3_0(S, a0, a1, a2, r0, r1, r2);
+      if (code == 1) {
+        r0 = r0 + L[0];
+        r1 = r1 + L[1];
+        r2 = r2 + L[2];
+      }
+    }
+  }
+  const double s_pos = r2;
+  const double rel_p = 1 + p.pz;
+  const double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+  if (pz <= 0) {
+    p.state = LOST_PZ;
+  } else {
+    double q0, q1, q2;
+    mv3_0(W, p.px, p.py, 1 * sqrt(pz), q0, q1, q2);
+    p.px = q0;
+    p.py = q1;
+    p.x = r0;
+    p.y = r1;
+  }
+  const double ds = (set ? 0.0 : 2 * L_half) - s_pos;
+  if (fabs(ds) > 1e-14 && p.state == ALIVE) track_a_drift<false>(p, ds, G, m);
+}
+
 // sbend_body_with_k1_map, track_a_bend.f90:500-659 (no matrix)
 __device__ __forceinline__ void sbend_k1_body(Part& p, const double* q) {
   const double g = q[B_G];
@@ -410,8 +513,9 @@ __device__ __forceinline__ void sbend_k1_body(Part& p, const double* q) {
         z33 * (r2 * r2) + z34 * r2 * r3 + z44 * (r3 * r3);
 }
 
-// Returns false when the element ends the particle (lost inside and
-// track_a_bend returns early).  bmad/low_level/track_a_bend.f90:18-333.
+// bmad/low_level/track_a_bend.f90:18-333.  With RARE: misaligned bends
+// (offset_particle's bend geometry) and electric multipoles.
+template <bool RARE>
 __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, DriftMemo& m) {
   const double* q = R.kb;
   const int32_t fl = R.h->flags;
@@ -419,10 +523,23 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
   const int n_step = R.h->n_step;
   const double* an = q + B_N;
   const double* bn = an + (ix + 1);
-  if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
-  if (fl & F_EDGE_IN) hwang_edge<true>(p, q + B_EDGE);
+  const int ixe = RARE ? R.h->aux1 : -1;
+  const double* ae = an + 2 * (ix + 1);
+  const double* be = ae + (ixe + 1);
+  if (fl & F_MISALIGN) {
+    if (RARE && (fl & F_BEND_MIS))
+      bend_offset(p, R.mis + MIS_N, true, R.mis[MIS_LHALF], G, m);
+    else
+      offset_set(p, R.mis, fl, G, m, true);
+  }
+  if (fl & F_EDGE_IN) {
+    // apply_element_edge_kick.f90:160-201: entering, magnetic then electric
+    hwang_edge<true>(p, q + B_EDGE);
+    if (RARE && (fl & F_ELEC_EDGE)) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
+  }
   if (orbit_too_large(p, G)) return;
   if (ix > -1) bend_multipole_kicks(p, q, an, bn, ix, 0.5, G);
+  if (RARE && ixe > -1) bend_elec_kicks(p, ae, be, ixe, 0.5, q[B_STEP], q[B_G], G);
   const double g = q[B_G];
   const double step_len = q[B_STEP];
   for (int n = 1; n <= n_step; n++) {
@@ -488,10 +605,20 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
       }
     }
     if (ix > -1) bend_multipole_kicks(p, q, an, bn, ix, (n == n_step) ? 0.5 : 1.0, G);
+    if (RARE && ixe > -1) bend_elec_kicks(p, ae, be, ixe, (n == n_step) ? 0.5 : 1.0, step_len, g, G);
   }
   if (orbit_too_large(p, G)) return;
-  if (fl & F_EDGE_OUT) hwang_edge<false>(p, q + B_EDGE + EDGE_N);
-  if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
+  if (fl & F_EDGE_OUT) {
+    // leaving: electric then magnetic
+    if (RARE && (fl & F_ELEC_EDGE)) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+    hwang_edge<false>(p, q + B_EDGE + EDGE_N);
+  }
+  if (fl & F_MISALIGN) {
+    if (RARE && (fl & F_BEND_MIS))
+      bend_offset(p, R.mis + MIS_N, false, R.mis[MIS_LHALF], G, m);
+    else
+      offset_unset(p, R.mis, fl, G, m, true);
+  }
 }
 
 // track1, bmad/code/track1.f90:43-342 for one alive particle and one record:
@@ -499,7 +626,7 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
 // particle's state (ALIVE or a lost code).
 template <bool RARE>
 __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glob& G, DriftMemo& m, QMemo qm) {
-  Rec R = decode(rec);
+  Rec R = decode<RARE>(rec);
   const int32_t fl = R.h->flags;
   if ((fl & F_AP_ENTRANCE) && G.ap_on) {
     if (RARE)
@@ -516,7 +643,7 @@ __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glo
       body_quad<RARE>(p, R, G, m, qm);
       break;
     case K_BEND:
-      body_bend(p, R, G, m);
+      body_bend<RARE>(p, R, G, m);
       break;
     case K_THICK_MULT:
       body_thick<RARE>(p, R, G, m);

@@ -45,8 +45,8 @@ enum Flag : int32_t {
   // quadrupole / thick multipole: init_fringe_info is true (a fringe type or
   // electric multipoles): the state is checked after each edge kick
   F_FRINGE_INFO = 1 << 15,
-  // quadrupole / thick multipole: electric multipoles, ae[aux1+1] and
-  // be[aux1+1] follow the magnetic an/bn arrays.  For these kinds
+  // quadrupole / thick multipole / bend: electric multipoles, ae[aux1+1]
+  // and be[aux1+1] follow the magnetic an/bn arrays.  For these kinds
   // F_EDGE_IN / F_EDGE_OUT mark the ends fringe_at names
   F_ELEC = 1 << 16,
   // the electric longitudinal fringe acts (electric multipoles, length != 0)
@@ -59,6 +59,10 @@ enum Flag : int32_t {
   // (collimators)
   F_AP_OFFSET = 1 << 19,
   F_AP_TILT = 1 << 20,
+  // misaligned bend with g, ref_tilt or roll nonzero: offset_particle's bend
+  // geometry (offset_particle.f90:208-235, 393-425), a bend-misalignment
+  // block (BM_*) after the misalignment block
+  F_BEND_MIS = 1 << 21,
 };
 
 struct RecHdr {
@@ -78,6 +82,7 @@ constexpr int HDR_DW = 4;
 // ---- parameter offsets (in doubles, relative to the record start) ----
 // Common blocks appear in this order after the header when their flag is set:
 //   misalignment block (F_MISALIGN):      MIS_N doubles
+//   bend-misalignment block (F_BEND_MIS): BM_N doubles
 //   aperture block (F_AP_*):              AP_N doubles
 // then the kind block.
 constexpr int MIS_XOFF = 0, MIS_YOFF = 1, MIS_ZOFF = 2, MIS_LHALF = 3, MIS_COS = 4, MIS_SIN = 5;
@@ -92,6 +97,22 @@ constexpr int MIS_ZADD = 30;      // z_offset + L/2 on unset
 constexpr int MIS_COSU = 31, MIS_SINU = 32;  // cos/sin of -tilt (unset)
 constexpr int MIS_R3EXIT = 33;    // 0 - (z_offset + ds_center) with s = L (aperture at the exit)
 constexpr int MIS_N = 34;
+
+// Bend-misalignment block (F_BEND_MIS).  The position (x, y, 0) goes through
+// a short list of affine steps with element-constant matrices -- the
+// bend_shift / misalignment / tilt frames offset_particle chains -- and the
+// momentum (px, py, ps) through the product W of their matrices:
+//   op (BM_OP_N doubles): [code, S (9, row-major), L (3)]
+//   code 0: r3 = r3 - L3        (bend_shift with zero angle)
+//   code 1: r = S r + L         (bend_shift; unset misalignment S r + L_mis)
+//   code 2: r = S (r - L)       (set misalignment S^T (r - L_mis))
+//   code 3: r = S r             (w_mat_for_tilt)
+//   code 4: r3 = r3 + L3
+constexpr int BM_NSET = 0, BM_NUNSET = 1;
+constexpr int BM_WSET = 2, BM_WUNSET = 11;  // 9 doubles each, row-major
+constexpr int BM_OP_N = 13, BM_MAX_OPS = 7;
+constexpr int BM_OPS_SET = 20, BM_OPS_UNSET = BM_OPS_SET + BM_MAX_OPS * BM_OP_N;
+constexpr int BM_N = BM_OPS_UNSET + BM_MAX_OPS * BM_OP_N;
 
 constexpr int AP_X1 = 0, AP_X2 = 1, AP_Y1 = 2, AP_Y2 = 3;  // x1_lim = -x1_limit, ...
 constexpr int AP_XW = 4, AP_XC = 5, AP_YW = 6, AP_YC = 7;  // elliptical width2/center

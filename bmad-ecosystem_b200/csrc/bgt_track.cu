@@ -73,6 +73,194 @@ static void w_mats(double theta, double phi, double w[9], double winv[9]) {
   winv[8] = c_the * c_phi;
 }
 
+// ---- bend geometry of offset_particle (F_BEND_MIS) ----
+// offset_particle.f90:208-235 (set) and :393-425 (unset) for a misaligned
+// bend, recorded as the affine steps of the BM block.  The matrices and
+// vectors are computed by the same steps, in the same floating-point order,
+// as the oracle's bend_offset_position; the device applies them to (x, y, 0).
+enum { AX_X = 0, AX_Y = 1, AX_Z = 2 };
+
+// sim_utils/special_functions/cos_one.f90:16-26
+static double cos_one_h(double angle) {
+  double s = sin(angle / 2);
+  return -(2 * (s * s));
+}
+
+// rotate_vec, sim_utils/math/rotation_3d_mod.f90:737-760
+static void rotate_vec_h(double v[3], int axis, double angle) {
+  if (angle == 0) return;
+  double ca = cos(angle), sa = sin(angle), a, b;
+  if (axis == AX_X) {
+    a = ca * v[1] - sa * v[2];
+    b = sa * v[1] + ca * v[2];
+    v[1] = a;
+    v[2] = b;
+  } else if (axis == AX_Y) {
+    a = sa * v[2] + ca * v[0];
+    b = ca * v[2] - sa * v[0];
+    v[0] = a;
+    v[2] = b;
+  } else {
+    a = ca * v[0] - sa * v[1];
+    b = sa * v[0] + ca * v[1];
+    v[0] = a;
+    v[1] = b;
+  }
+}
+
+// rotate_mat without right_multiply (mat = Rot . mat),
+// rotation_3d_mod.f90:781-835: every column as rotate_vec
+static void rotate_mat_h(double m[3][3], int axis, double angle) {
+  if (angle == 0) return;
+  for (int j = 0; j < 3; j++) {
+    double v[3] = {m[0][j], m[1][j], m[2][j]};
+    rotate_vec_h(v, axis, angle);
+    m[0][j] = v[0];
+    m[1][j] = v[1];
+    m[2][j] = v[2];
+  }
+}
+
+// 3x3 matmul with k-ordered sums from zero (gfortran's inline matmul)
+static void matmul33_h(const double a[3][3], const double b[3][3], double out[3][3]) {
+  double t[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0;
+      for (int k = 0; k < 3; k++) s = s + a[i][k] * b[k][j];
+      t[i][j] = s;
+    }
+  memcpy(out, t, sizeof(t));
+}
+
+// floor_angles_to_w_mat (not inverse), floor_angles_to_w_mat.f90:17-57
+static void floor_w_h(double theta, double phi, double psi, double w[3][3]) {
+  double s_the = sin(theta), c_the = cos(theta);
+  double s_phi = sin(phi), c_phi = cos(phi);
+  double s_psi = sin(psi), c_psi = cos(psi);
+  w[0][0] = c_the * c_psi - s_the * s_phi * s_psi;
+  w[0][1] = -c_the * s_psi - s_the * s_phi * c_psi;
+  w[0][2] = s_the * c_phi;
+  w[1][0] = c_phi * s_psi;
+  w[1][1] = c_phi * c_psi;
+  w[1][2] = s_phi;
+  w[2][0] = -s_the * c_psi - c_the * s_phi * s_psi;
+  w[2][1] = s_the * s_psi - c_the * s_phi * c_psi;
+  w[2][2] = c_the * c_phi;
+}
+
+struct BendChain {
+  double* ops;
+  int n = 0;
+  double W[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  explicit BendChain(double* o) : ops(o) {}
+  void op(int code, const double S[3][3], const double L[3]) {
+    double* o = ops + n * BM_OP_N;
+    o[0] = code;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) o[1 + 3 * i + j] = S[i][j];
+    for (int i = 0; i < 3; i++) o[10 + i] = L[i];
+    if (code >= 1 && code <= 3) matmul33_h(S, W, W);
+    n++;
+  }
+  // bend_shift, bmad/geometry/bend_shift.f90:19-61 (has_tilt: ref_tilt given)
+  void shift(double g, double delta_s, bool has_tilt, double ref_tilt) {
+    const double I[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    double angle = delta_s * g;
+    if (angle == 0) {
+      const double L[3] = {0.0, 0.0, delta_s};
+      op(0, I, L);
+      return;
+    }
+    double tlt = has_tilt ? ref_tilt : 0.0;
+    double S[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    if (tlt != 0) {
+      rotate_mat_h(S, AX_Z, -ref_tilt);
+      rotate_mat_h(S, AX_Y, angle);
+      rotate_mat_h(S, AX_Z, ref_tilt);
+    } else {
+      rotate_mat_h(S, AX_Y, angle);
+    }
+    double L[3] = {cos_one_h(angle) / g, 0.0 / g, -sin(angle) / g};
+    if (has_tilt) rotate_vec_h(L, AX_Z, ref_tilt);
+    op(1, S, L);
+  }
+};
+
+// ele_misalignment_L_S_calc, bmad/geometry/ele_misalignment_L_S_calc.f90:
+// 16-50, sbend branch (angle = g L, rho = 1/g)
+static void bend_L_S(const bgt_element& e, double L_mis[3], double S[3][3]) {
+  L_mis[0] = e.x_offset;
+  L_mis[1] = e.y_offset;
+  L_mis[2] = e.z_offset;
+  if (e.roll != 0) {
+    double angle = e.g * e.l;
+    double rho = e.g == 0 ? 0.0 : 1 / e.g;
+    double Lc[3] = {rho * cos_one_h(angle / 2), rho * 0.0, rho * sin(angle / 2)};
+    rotate_vec_h(Lc, AX_Y, angle / 2);
+    rotate_vec_h(Lc, AX_Z, e.ref_tilt);
+    for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] - Lc[i];
+    rotate_vec_h(Lc, AX_Z, e.roll);
+    for (int i = 0; i < 3; i++) L_mis[i] = L_mis[i] + Lc[i];
+  }
+  floor_w_h(e.x_pitch, e.y_pitch, e.roll, S);
+}
+
+// w_mat_for_tilt, bmad/geometry/w_mat_for_tilt.f90:13-40 (not inverse)
+static void w_tilt_h(double tilt, double w[3][3]) {
+  double c = cos(tilt), s = sin(tilt);
+  const double t[3][3] = {{c, -s, 0.0}, {s, c, 0.0}, {0.0, 0.0, 1.0}};
+  memcpy(w, t, sizeof(t));
+}
+
+// The BM block: the set chain (drift to the entrance edge) and the unset
+// chain (drift to the exit edge).
+static void bend_mis_block(const bgt_element& e, double* bm) {
+  const double g = e.g, rt = e.ref_tilt, L = e.l, L_half = 0.5 * L;
+  const double I[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  const double zero[3] = {0.0, 0.0, 0.0};
+  double L_mis[3], ws[3][3], wt[3][3], wm[3][3];
+  bend_L_S(e, L_mis, ws);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
+  {
+    BendChain c(bm + BM_OPS_SET);
+    const double ds_center = L_half - 0.0;
+    c.shift(g, 1 * ds_center, true, rt);
+    c.op(2, wt, L_mis);
+    if (rt != 0) {
+      c.shift(g, -L_half, true, rt);
+      w_tilt_h(-rt, wm);
+      c.op(3, wm, zero);
+      c.shift(g, L_half, false, 0.0);
+    }
+    c.shift(g, -1 * 1 * L_half, false, 0.0);
+    const double add[3] = {0.0, 0.0, (1 - 1 * 1) * L_half};
+    c.op(4, I, add);
+    bm[BM_NSET] = c.n;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) bm[BM_WSET + 3 * i + j] = c.W[i][j];
+  }
+  {
+    BendChain c(bm + BM_OPS_UNSET);
+    const double ds_center = L_half - L;
+    c.shift(g, ds_center, false, 0.0);
+    if (rt != 0) {
+      c.shift(g, -L_half, false, 0.0);
+      w_tilt_h(rt, wm);
+      c.op(3, wm, zero);
+      c.shift(g, L_half, true, rt);
+    }
+    c.op(1, ws, L_mis);
+    c.shift(g, 1 * 1 * L_half, true, rt);
+    const double add[3] = {0.0, 0.0, (1 + 1 * 1) * L_half};
+    c.op(4, I, add);
+    bm[BM_NUNSET] = c.n;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) bm[BM_WUNSET + 3 * i + j] = c.W[i][j];
+  }
+}
+
 struct Builder {
   std::vector<double>& out;
   size_t start;
@@ -136,8 +324,8 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
                            std::string& err) {
   const int ixe = max_nonzero(e.an_elec, e.bn_elec, BGT_N_POLE);
   if (ixe > -1 && e.is_on && e.key != BGT_QUADRUPOLE && e.key != BGT_SEXTUPOLE && e.key != BGT_OCTUPOLE &&
-      e.key != BGT_THICK_MULTIPOLE) {
-    err = ename(e) + ": electric multipoles are supported on quadrupoles and thick multipoles only";
+      e.key != BGT_THICK_MULTIPOLE && e.key != BGT_SBEND) {
+    err = ename(e) + ": electric multipoles are supported on quadrupoles, bends and thick multipoles only";
     return BGT_EUNSUPPORTED;
   }
   if (e.p0c != p0c) {
@@ -176,7 +364,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
   // ---- misalignment (offset_particle) ----
   bool offset = e.x_offset != 0 || e.y_offset != 0 || e.z_offset != 0 || e.x_pitch != 0 || e.y_pitch != 0;
   bool pitch = e.x_pitch != 0 || e.y_pitch != 0;
-  bool use_mis = false;
+  bool use_mis = false, bend_mis = false;
   double tilt = 0;
   if (kind == K_QUAD || kind == K_THICK_MULT || kind == K_THIN_MULT) {
     use_mis = e.has_misalign != 0;
@@ -185,17 +373,22 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     use_mis = true;  // track_a_rfcavity calls offset_particle unconditionally
     tilt = e.tilt;
   } else if (kind == K_BEND) {
-    if (offset || e.roll != 0) {
-      err = ename(e) + ": bend offsets/pitches/roll are not supported";
-      return BGT_EUNSUPPORTED;
+    // is_misaligned, offset_particle.f90:195-196
+    const bool misaligned = offset || e.roll != 0;
+    if (misaligned && (e.g != 0 || e.ref_tilt != 0 || e.roll != 0)) {
+      use_mis = bend_mis = true;  // the bend geometry (BM block)
+    } else if (misaligned) {
+      use_mis = true;  // g = ref_tilt = roll = 0: the straight-element geometry
+    } else {
+      use_mis = e.has_misalign != 0 && e.ref_tilt != 0;
+      tilt = e.ref_tilt;
     }
-    use_mis = e.has_misalign != 0 && e.ref_tilt != 0;
-    tilt = e.ref_tilt;
   }
   if (use_mis) {
     flags |= F_MISALIGN;
-    if (offset) flags |= F_OFFSET;
-    if (pitch) flags |= F_PITCH;
+    if (bend_mis) flags |= F_BEND_MIS;
+    if (offset && !bend_mis) flags |= F_OFFSET;
+    if (pitch && !bend_mis) flags |= F_PITCH;
     if (tilt != 0 && kind != K_THIN_MULT) flags |= F_TILT;
     if (kind == K_RFCAVITY && e.is_on && (e.hkick != 0 || e.vkick != 0)) flags |= F_HV_KICK;
   }
@@ -255,6 +448,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     m[MIS_R3EXIT] = 0.0 - (e.z_offset + 1 * ds_center_exit);
     double s_lab = m[MIS_R3UNSET] + m[MIS_ZADD];
     m[MIS_DS_UNSET] = (1 + 1) * L_half - s_lab;
+    if (flags & F_BEND_MIS) bend_mis_block(e, B.ptr_after_push(BM_N));
   }
   if (flags & (F_AP_ENTRANCE | F_AP_EXIT)) {
     double* a = B.ptr_after_push(AP_N);
@@ -387,6 +581,10 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
         err = ename(e) + ": bend fringe_type other than basic_bend/hard_edge_only is not supported";
         return BGT_EUNSUPPORTED;
       }
+      if (ixe > -1 && !edges && e.fringe_at != BGT_NO_END) {
+        err = ename(e) + ": electric multipoles on a bend with fringe_type none are not supported";
+        return BGT_EUNSUPPORTED;
+      }
       // multipole_ele_to_ab(..., include_kicks$, b1) then track_a_bend.f90:58-94
       double b1 = bn[1];
       bn[1] = 0;
@@ -411,7 +609,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
         b1 = 0;
       }
       int n_step = 1;
-      if (ix > -1) n_step = std::max(nint_h(fabs(length) / e.ds_step), 1);
+      if (ix > -1 || ixe > -1) n_step = std::max(nint_h(fabs(length) / e.ds_step), 1);
       double r_step = 1.0 / n_step;
       double step_len = length / n_step;
       double angle = g * step_len;
@@ -469,6 +667,19 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     }
   }
   h.aux1 = -1;
+  if (kind == K_BEND && ixe > -1) {
+    // electric multipoles of a bend: kicks in apply_multipole_kicks
+    // (track_a_bend.f90:379-466), longitudinal fringe at the ends the Hwang
+    // edges act (apply_element_edge_kick.f90:160-163)
+    flags |= F_ELEC;
+    h.aux1 = ixe;
+    double* q = B.ptr_after_push(2 * (ixe + 1));
+    for (int n = 0; n <= ixe; n++) {
+      q[n] = e.an_elec[n];
+      q[ixe + 1 + n] = e.bn_elec[n];
+    }
+    if (e.l != 0) flags |= F_ELEC_EDGE;
+  }
   if (kind == K_QUAD || kind == K_THICK_MULT) {
     // init_fringe_info (bmad/low_level/init_fringe_info.f90:22-60); the edge
     // kicks act at the ends fringe_at names (apply_element_edge_kick.f90:104)
@@ -633,7 +844,9 @@ static cudaError_t upload_multipole_tables() {
 }
 
 // Whether a compiled record uses a feature only the RARE kernels handle.
-static bool record_is_rare(const RecHdr* rh) { return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET)) != 0; }
+static bool record_is_rare(const RecHdr* rh) {
+  return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS)) != 0;
+}
 
 // Enqueue tracking of slots on `st`.
 static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t st) {

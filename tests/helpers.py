@@ -79,6 +79,35 @@ def zoo_lattice(apertures: bool = True) -> L.Lattice:
     return lat.finalize()
 
 
+def rare_zoo_lattice() -> L.Lattice:
+    """Element forms that only the device's RARE kernels handle: misaligned
+    bends (offset_particle's bend geometry, with g, ref_tilt or roll), the
+    straight geometry of a misaligned g = 0 bend, electric multipoles in bends
+    and quadrupoles, the hard-edge multipole fringe and a misaligned
+    collimator whose aperture moves with it -- at the 5 GeV ring energy."""
+    E = []
+    E.append(L.Element("drift", "D", {"l": 0.5}))
+    E.append(L.Element("sbend", "BMIS", {"l": 1.0, "g": 0.02, "e1": 0.03, "e2": 0.01, "x_offset": 1e-4,
+                                         "y_offset": -2e-4, "z_offset": 1e-3, "x_pitch": 1e-4, "y_pitch": -2e-4,
+                                         "ref_tilt": 0.05}))
+    E.append(L.Element("sbend", "BROLL", {"l": 1.5, "g": 0.015, "roll": 2e-3, "x_offset": 1e-4}))
+    E.append(L.Element("sbend", "BSTRAIGHT", {"l": 0.8, "k1": 0.1, "x_offset": 1e-4, "y_pitch": 1e-4}))
+    E.append(L.Element("sbend", "BG0TILT", {"l": 0.8, "k1": 0.15, "ref_tilt": 0.1, "y_offset": 1e-4}))
+    E.append(L.Element("sbend", "BELEC", {"l": 1.0, "g": 0.01, "e1": 0.05}, b_pole_elec={0: 2e4, 1: 5e6},
+                       a_pole_elec={2: 1e8}))
+    E.append(L.Element("sbend", "BELECMIS", {"l": 0.6, "g": 0.01, "e1": 0.1, "e2": 0.2, "x_offset": 2e-4,
+                                             "y_pitch": 1e-4, "ref_tilt": 0.1, "vkick": -1e-5, "r0_mag": 2.0,
+                                             "r0_elec": 3.0}, num_steps=10,
+                       a_pole={0: 1e-4, 1: 1e-3}, a_pole_elec={1: 2e6}, b_pole_elec={0: -2e5}))
+    E.append(L.Element("quadrupole", "QELEC", {"l": 0.4, "k1": 0.7, "x_offset": 1e-4, "tilt": 0.01},
+                       num_steps=4, fringe_type="full", a_pole_elec={1: 3e6}, b_pole_elec={0: 1e5}))
+    E.append(L.Element("sextupole", "SHARD", {"l": 0.2, "k2": 30.0}, fringe_type="hard_edge_only"))
+    E.append(L.Element("ecollimator", "ECMIS", {"l": 0.2, "x1_limit": 0.015, "x2_limit": 0.0165, "y1_limit": 0.01,
+                                                "y2_limit": 0.01, "x_offset": 5e-4, "tilt": 0.2}))
+    lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "rare_zoo")
+    return lat.finalize()
+
+
 def random_particles(n: int, seed: int, scale: float = 1.0) -> np.ndarray:
     """Particles spanning a few mm / mrad / percent: (6, n)."""
     rng = np.random.Generator(np.random.Philox(seed))

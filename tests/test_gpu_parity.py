@@ -19,7 +19,7 @@ from bgt import rings
 from bgt.track import Bunch, Tracker
 
 from helpers import (RTOL_1000_TURNS, RTOL_LIBM_1000_TURNS, RTOL_LIBM_ONE_TURN, RTOL_ONE_TURN,
-                     oracle_track_elements, random_particles, rel_err, zoo_lattice)
+                     oracle_track_elements, random_particles, rare_zoo_lattice, rel_err, zoo_lattice)
 
 pytestmark = pytest.mark.gpu
 
@@ -70,6 +70,39 @@ def test_zoo_pass_with_losses(zoo):
     ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, 0, len(lat), variant="cr")
     assert (ost != L.ALIVE).sum() > 100  # the case exercises losses
     assert_bitwise(b, ov, ob, ost, oie, what="zoo pass")
+
+
+@pytest.fixture(scope="module")
+def rare_zoo():
+    lat = rare_zoo_lattice()
+    return lat, Tracker(lat)
+
+
+def test_rare_zoo_each_element_bitwise(rare_zoo):
+    # misaligned and electric bends, electric quadrupoles, edge fringe and
+    # element-frame apertures: the RARE kernels against the oracle
+    lat, tr = rare_zoo
+    v0 = random_particles(2048, seed=21)
+    for pos, ele in enumerate(lat.elements):
+        b = tr.make_bunch(v0.copy())
+        tr.track1(b, pos)
+        ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
+        assert_bitwise(b, ov, ob, ost, oie, what=ele.name)
+        ovg, _, ostg, _, _ = oracle_track_elements(lat, v0, pos, pos + 1)
+        assert np.array_equal(b.state, ostg), f"{ele.name}: state vs glibc oracle"
+        assert np.all(rel_err(b.vec6, ovg, ostg == L.ALIVE) <= RTOL_ONE_TURN), ele.name
+
+
+def test_rare_zoo_turns_with_losses(rare_zoo):
+    lat, tr = rare_zoo
+    # the line does not close, so the orbit grows turn by turn: particles are
+    # lost at the collimator over all five turns
+    v0 = random_particles(4096, seed=22)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, 5)
+    ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), 5, variant="cr")
+    assert len(np.unique(oit[ost != L.ALIVE])) == 5 and (ost == L.ALIVE).sum() > 0
+    assert_bitwise(b, ov, ob, ost, oie, oit, what="rare zoo, 5 turns")
 
 
 @pytest.fixture(scope="module")
