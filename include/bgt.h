@@ -42,8 +42,11 @@
  *    by the caller (the *_device entry points).
  *
  * Scope: forward tracking (direction = time_dir = orientation = +1), relative
- * RF time (bmad_com%absolute_time_tracking = F), magnetic multipoles, no
- * radiation/spin.  bgt_create rejects any element outside that scope with
+ * RF time (bmad_com%absolute_time_tracking = F), magnetic and electric
+ * multipoles (electric ones on quadrupoles, sextupoles, octupoles, thick
+ * multipoles and bends), misaligned elements including bends, no
+ * radiation/spin, no exact bend multipoles, no full / soft bend fringe, no RF
+ * coupler kick.  bgt_create rejects any element outside that scope with
  * BGT_EUNSUPPORTED and names the element.
  */
 #ifndef BGT_H
