@@ -24,13 +24,14 @@ BGT_OK, BGT_EINVAL, BGT_EUNSUPPORTED, BGT_ECUDA, BGT_ENOMEM, BGT_ETIMEOUT, BGT_E
 class BgtElement(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "key", "ix_ele", "is_on", "num_steps", "fringe_type", "fringe_at", "aperture_type", "aperture_at",
-        "offset_moves_aperture", "exact_multipoles", "has_misalign", "reserved")] + [
+        "offset_moves_aperture", "exact_multipoles", "has_misalign", "coupler_at")] + [
         (n, C.c_double) for n in (
             "l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
             "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset",
             "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",
             "x1_limit", "x2_limit", "y1_limit", "y2_limit")] + [
-        (n, C.c_double * N_POLE) for n in ("an", "bn", "an_elec", "bn_elec", "knl", "tn")]
+        (n, C.c_double * N_POLE) for n in ("an", "bn", "an_elec", "bn_elec", "knl", "tn")] + [
+        ("coupler_angle", C.c_double), ("coupler_phase", C.c_double)]
 
 
 class BgtSpecies(C.Structure):
@@ -115,6 +116,9 @@ def to_bgt_element(e: L.Element) -> BgtElement:
     b.offset_moves_aperture = 1 if e.offset_moves_aperture else 0
     b.exact_multipoles = e.exact_multipoles
     b.has_misalign = 1 if e.has_misalign else 0
+    b.coupler_at = L.ENDS[e.coupler_at]
+    b.coupler_angle = e.v("coupler_angle")
+    b.coupler_phase = e.v("coupler_phase")
     for n in ("l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
               "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset",
               "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",

@@ -60,7 +60,7 @@ _VALUE_NAMES = [
     "l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
     "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset", "y_offset",
     "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick", "x1_limit",
-    "x2_limit", "y1_limit", "y2_limit", "r0_mag", "r0_elec",
+    "x2_limit", "y1_limit", "y2_limit", "r0_mag", "r0_elec", "coupler_angle", "coupler_phase",
 ]
 
 
@@ -129,6 +129,8 @@ class Element:
     ix_ele: int = 0
     user_num_steps: Optional[int] = None
     user_ds_step: Optional[float] = None
+    # rfcavity: the ends with a coupler kick (set_ele_defaults.f90:309)
+    coupler_at: str = "exit_end"
 
     def __post_init__(self):
         if self.key == "rbend":
@@ -154,7 +156,7 @@ class Element:
                     self.fringe_at, self.aperture_type, self.aperture_at, self.offset_moves_aperture,
                     self.exact_multipoles, self.scale_multipoles, dict(self.a_pole), dict(self.b_pole),
                     dict(self.ksl_pole), dict(self.a_pole_elec), dict(self.b_pole_elec), self.has_misalign,
-                    self.ix_ele, self.user_num_steps, self.user_ds_step)
+                    self.ix_ele, self.user_num_steps, self.user_ds_step, self.coupler_at)
         return e
 
     @property

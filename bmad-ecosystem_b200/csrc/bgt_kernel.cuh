@@ -280,6 +280,23 @@ __device__ __forceinline__ DD dd_modulo2(double x, DD amp) {
 }
 
 // bmad/low_level/track_a_rfcavity.f90:17-146, relative time, no coupler
+// rf_coupler_kick, bmad/low_level/rf_coupler_kick.f90:20-104 (tracking part)
+// for an rfcavity: ph = pi/2 - phase + twopi * coupler_phase, the transverse
+// kick dp cos(ph) / p0c and the energy change (dp_x x + dp_y y) f2.
+__device__ __forceinline__ void rf_coupler_kick(Part& p, const double* q, double phase, const Glob& G) {
+  double ph = phase;
+  ph = PI_D / 2 - ph;
+  ph = ph + q[RF_CPL_PH];
+  const double dp_x = q[RF_CPL_DPX], dp_y = q[RF_CPL_DPY];
+  const double c = cr::cos(ph);
+  p.px = p.px + 1 * dp_x * c / G.p0c;
+  p.py = p.py + 1 * dp_y * c / G.p0c;
+  const double f2 = 1 * cr::sin(ph) * TWOPI_D * q[RF_FREQ] / C_LIGHT;
+  const double dE = (dp_x * p.x + dp_y * p.y) * f2;
+  apply_energy_kick(p, dE, G);
+}
+
+template <bool RARE>
 __device__ __forceinline__ void body_rf(Part& p, const Rec& R, const Glob& G, DriftMemo& m) {
   const double* q = R.kb;
   const int32_t fl = R.h->flags;
@@ -305,6 +322,7 @@ __device__ __forceinline__ void body_rf(Part& p, const Rec& R, const Glob& G, Dr
   if (mod != 0 && ((mod < 0) != (per < 0))) mod += per;
   if (mod >= PI_D) mod = mod - per;
   double phase = mod;
+  if (RARE && (fl & F_COUPLER_IN)) rf_coupler_kick(p, q, phase, G);
   const int n_slice = R.h->n_step;
   const double slice_l = q[RF_SLICE_L];
   for (int i = 0; i <= n_slice; i++) {
@@ -321,6 +339,7 @@ __device__ __forceinline__ void body_rf(Part& p, const Rec& R, const Glob& G, Dr
       phase = phase + q[RF_TWOPI_F] * (p.z - z0) / (C_LIGHT * p.beta);
     }
   }
+  if (RARE && (fl & F_COUPLER_OUT)) rf_coupler_kick(p, q, phase, G);
   if (ix > -1) ab_multipole_kicks(p, an, bn, ix, q[RF_RHALF]);
   offset_unset(p, R.mis, fl, G, m, true);
 }
@@ -652,7 +671,7 @@ __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glo
       body_thin(p, R, G, m);
       break;
     case K_RFCAVITY:
-      body_rf(p, R, G, m);
+      body_rf<RARE>(p, R, G, m);
       break;
     default:
       break;

@@ -63,6 +63,9 @@ enum Flag : int32_t {
   // geometry (offset_particle.f90:208-235, 393-425), a bend-misalignment
   // block (BM_*) after the misalignment block
   F_BEND_MIS = 1 << 21,
+  // rfcavity coupler kick at the entrance / exit (rf_coupler_kick.f90)
+  F_COUPLER_IN = 1 << 22,
+  F_COUPLER_OUT = 1 << 23,
 };
 
 struct RecHdr {
@@ -167,7 +170,9 @@ constexpr int RF_TWOPI_F = 6;  // twopi * rf_frequency
 constexpr int RF_HALF_AMP_HI = 7, RF_HALF_AMP_LO = 8;  // 0.5/f as double-double
 constexpr int RF_PHI0_MP = 9;  // twopi * phi0_multipass
 constexpr int RF_RHALF = 10;   // 0.5 * r_step (multipole kicks)
-constexpr int RF_N = 11;
+constexpr int RF_CPL_DPX = 11, RF_CPL_DPY = 12;  // coupler dp_x, dp_y (halved for both ends)
+constexpr int RF_CPL_PH = 13;  // twopi * coupler_phase
+constexpr int RF_N = 14;
 
 // Multipole arrays for quad / bend / thick multipole / rf follow the kind
 // block: an[0..ix_mag_max], bn[0..ix_mag_max].

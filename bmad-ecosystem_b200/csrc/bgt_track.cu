@@ -539,10 +539,6 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       break;
     }
     case K_RFCAVITY: {
-      if (e.coupler_strength != 0) {
-        err = ename(e) + ": rf coupler kicks are not supported";
-        return BGT_EUNSUPPORTED;
-      }
       if (e.rf_frequency == 0 && e.voltage != 0) {
         err = ename(e) + ": rfcavity has zero rf_frequency";
         return BGT_EINVAL;
@@ -567,6 +563,25 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       }
       q[RF_PHI0_MP] = TWOPI_H * e.phi0_multipass;
       q[RF_RHALF] = 0.5 * r_step;
+      // rf_coupler_kick.f90:41-60: e_accel_field(ele, gradient$) is voltage / l
+      // (attribute_bookkeeper.f90:730-736) times field_autoscale = 1
+      if (e.coupler_strength != 0) {
+        const int cat = e.coupler_at;
+        if (cat == BGT_ENTRANCE_END || cat == BGT_BOTH_ENDS) flags |= F_COUPLER_IN;
+        if (cat == BGT_EXIT_END || cat == BGT_BOTH_ENDS) flags |= F_COUPLER_OUT;
+        double gradient = e.voltage == 0 ? 0.0 : (e.l == 0 ? 1e30 : e.voltage / e.l);
+        double field = e.is_on ? gradient * 1.0 : 0.0;
+        double dp_coef = field * e.coupler_strength;
+        double dp_x = dp_coef * cos(TWOPI_H * e.coupler_angle);
+        double dp_y = dp_coef * sin(TWOPI_H * e.coupler_angle);
+        if (cat == BGT_BOTH_ENDS) {
+          dp_x = dp_x / 2;
+          dp_y = dp_y / 2;
+        }
+        q[RF_CPL_DPX] = dp_x;
+        q[RF_CPL_DPY] = dp_y;
+        q[RF_CPL_PH] = TWOPI_H * e.coupler_phase;
+      }
       h.n_step = n_slice;
       h.ix_mag_max = ix;
       break;
@@ -845,7 +860,7 @@ static cudaError_t upload_multipole_tables() {
 
 // Whether a compiled record uses a feature only the RARE kernels handle.
 static bool record_is_rare(const RecHdr* rh) {
-  return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS)) != 0;
+  return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS | F_COUPLER_IN | F_COUPLER_OUT)) != 0;
 }
 
 // Enqueue tracking of slots on `st`.

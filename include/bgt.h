@@ -44,9 +44,9 @@
  * Scope: forward tracking (direction = time_dir = orientation = +1), relative
  * RF time (bmad_com%absolute_time_tracking = F), magnetic and electric
  * multipoles (electric ones on quadrupoles, sextupoles, octupoles, thick
- * multipoles and bends), misaligned elements including bends, no
- * radiation/spin, no exact bend multipoles, no full / soft bend fringe, no RF
- * coupler kick.  bgt_create rejects any element outside that scope with
+ * multipoles and bends), misaligned elements including bends, RF coupler
+ * kicks, no radiation/spin, no exact bend multipoles, no full / soft bend
+ * fringe.  bgt_create rejects any element outside that scope with
  * BGT_EUNSUPPORTED and names the element.
  */
 #ifndef BGT_H
@@ -121,7 +121,7 @@ typedef struct bgt_element {
   int32_t offset_moves_aperture;
   int32_t exact_multipoles; /* 0 = off$ */
   int32_t has_misalign;     /* ele%bookkeeping_state%has_misalign */
-  int32_t reserved;
+  int32_t coupler_at;       /* rfcavity: coupler_at (end codes as fringe_at; default exit end) */
   double l, k1, k2, k3, g, dg, e1, e2, fint, hgap, fintx, hgapx;
   double voltage, phi0, phi0_multipass, rf_frequency, coupler_strength;
   double p0c, e_tot, ds_step;
@@ -131,6 +131,7 @@ typedef struct bgt_element {
   double an[BGT_N_POLE], bn[BGT_N_POLE];
   double an_elec[BGT_N_POLE], bn_elec[BGT_N_POLE];
   double knl[BGT_N_POLE], tn[BGT_N_POLE];
+  double coupler_angle, coupler_phase; /* rfcavity coupler (with coupler_strength) */
 } bgt_element;
 
 /* Tracked species (lat%param%particle) and bmad_com switches. */

@@ -234,6 +234,7 @@ void bgo_ele_init(bgo_ele* ele, int key) {
   if (key == BGO_RFCAVITY) {
     ele->fringe_type = BGO_FRINGE_FULL; /* set_ele_defaults.f90:315 */
     ele->num_steps = 10;                /* set_ele_defaults.f90:317 */
+    ele->coupler_at = BGO_EXIT_END;     /* set_ele_defaults.f90:309 */
   }
   if (key == BGO_RCOLLIMATOR || key == BGO_ECOLLIMATOR) ele->offset_moves_aperture = 1;
   ele->fintx = NAN; /* real_garbage$ until bookkeeping copies fint */
@@ -1999,6 +2000,38 @@ static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) 
   return 0;
 }
 
+/* rf_coupler_kick, bmad/low_level/rf_coupler_kick.f90:20-104 (tracking part)
+ * for an rfcavity: the coupler's transverse kick with the energy change it
+ * implies.  e_accel_field(ele, gradient$) = voltage / l (attribute_bookkeeper
+ * .f90:730-736) times field_autoscale = 1, the value bmad_standard tracking
+ * keeps (autoscale_phase_and_amp.f90:108-115). */
+static void rf_coupler_kick(const bgo_ele* ele, int first_edge, double phase, bgo_coord* orbit,
+                            const bgo_param* param) {
+  int physical_end = first_edge ? BGO_ENTRANCE_END : BGO_EXIT_END;
+  if (!(ele->coupler_at == BGO_BOTH_ENDS || ele->coupler_at == physical_end)) return;
+  if (ele->coupler_strength == 0) return;
+  double ph = phase;
+  ph = PI / 2 - ph;
+  ph = ph + TWOPI * ele->coupler_phase;
+  double gradient = ele->voltage == 0 ? 0.0 : (ele->l == 0 ? 1e30 : ele->voltage / ele->l);
+  double field = ele->is_on ? gradient * 1.0 : 0.0;
+  double dp_coef = field * ele->coupler_strength;
+  double dp_x = dp_coef * cos(TWOPI * ele->coupler_angle);
+  double dp_y = dp_coef * sin(TWOPI * ele->coupler_angle);
+  if (ele->coupler_at == BGO_BOTH_ENDS) {
+    dp_x = dp_x / 2;
+    dp_y = dp_y / 2;
+  }
+  double c = P_COS(ph);
+  orbit->vec[1] = orbit->vec[1] + 1 * dp_x * c / orbit->p0c;
+  orbit->vec[3] = orbit->vec[3] + 1 * dp_y * c / orbit->p0c;
+  double f2 = 1 * P_SIN(ph) * TWOPI * ele->rf_frequency / C_LIGHT;
+  double dE = (dp_x * orbit->vec[0] + dp_y * orbit->vec[2]) * f2;
+  LM(2);
+  FL(16);
+  apply_energy_kick(dE, orbit, param);
+}
+
 /* track_a_rfcavity, bmad/low_level/track_a_rfcavity.f90:17-146 with
  * particle_rf_time (bmad/code/particle_rf_time.f90:32-120) in relative-time
  * mode, rf_ref_time_offset = 0 (rf_ref_time_offset.f90:33) and no coupler
@@ -2035,6 +2068,7 @@ static int track_a_rfcavity(bgo_coord* orbit, const bgo_ele* ele, const bgo_para
   double phase = modulo2_dp(phase0, PI);
   LM(0);
   FL(8);
+  rf_coupler_kick(ele, 1, phase, orbit, param);
 
   for (int i = 0; i <= n_slice; i++) {
     double dE = 1 * voltage * P_SIN(phase) / n_slice;
@@ -2053,6 +2087,7 @@ static int track_a_rfcavity(bgo_coord* orbit, const bgo_ele* ele, const bgo_para
       FL(7);
     }
   }
+  rf_coupler_kick(ele, 0, phase, orbit, param);
   if (ix_elec_max > -1) ab_multipole_kicks(ae, be, ix_elec_max, ele, orbit, param, 1, 0.5 * step_len);
   if (ix_mag_max > -1) ab_multipole_kicks(an, bn, ix_mag_max, ele, orbit, param, 0, 0.5 * r_step);
   offset_particle(ele, 0, orbit, 1, 1, 0, 0, param);

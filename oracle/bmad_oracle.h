@@ -109,6 +109,7 @@ typedef struct bgo_ele {
   int scale_multipoles, field_master;
   int has_misalign;                  /* ele%bookkeeping_state%has_misalign (set by bgo_bookkeeper) */
   int num_steps;
+  int coupler_at; /* rfcavity: ends with the coupler kick */
   double l, k1, k2, k3, g, dg, e1, e2, fint, hgap, fintx, hgapx;
   double voltage, phi0, phi0_multipass, rf_frequency;
   double p0c, e_tot, ds_step;
@@ -118,6 +119,7 @@ typedef struct bgo_ele {
   double px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center;
   double z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center;
   double r0_mag, r0_elec;
+  double coupler_strength, coupler_angle, coupler_phase;
   /* For BGO_MULTIPOLE: a_pole = knl, b_pole = tn, ksl_pole = ksl (pointer_to_ele_multipole). */
   double a_pole[BGO_N_POLE], b_pole[BGO_N_POLE], ksl_pole[BGO_N_POLE];
   double a_pole_elec[BGO_N_POLE], b_pole_elec[BGO_N_POLE];

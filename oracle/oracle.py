@@ -41,12 +41,13 @@ class Coord(C.Structure):
 
 _INTS = ["key", "ix_ele", "is_on", "fringe_type", "fringe_at", "aperture_type", "aperture_at",
          "offset_moves_aperture", "has_mag_poles", "has_elec_poles", "scale_multipoles", "field_master",
-         "has_misalign", "num_steps"]
+         "has_misalign", "num_steps", "coupler_at"]
 _DBLS = ["l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
          "phi0_multipass", "rf_frequency", "p0c", "e_tot", "ds_step", "x_offset", "y_offset", "z_offset", "x_pitch",
          "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick", "x1_limit", "x2_limit", "y1_limit",
          "y2_limit", "px_aperture_width2", "px_aperture_center", "py_aperture_width2", "py_aperture_center",
-         "z_aperture_width2", "z_aperture_center", "pz_aperture_width2", "pz_aperture_center", "r0_mag", "r0_elec"]
+         "z_aperture_width2", "z_aperture_center", "pz_aperture_width2", "pz_aperture_center", "r0_mag", "r0_elec",
+         "coupler_strength", "coupler_angle", "coupler_phase"]
 
 
 class Ele(C.Structure):
@@ -116,6 +117,7 @@ def to_ele(e, lib=None, raw_bookkeeping: bool = False) -> Ele:
     o.aperture_type = APT[e.aperture_type]
     o.aperture_at = ENDS[e.aperture_at]
     o.offset_moves_aperture = 1 if e.offset_moves_aperture else 0
+    o.coupler_at = ENDS[getattr(e, "coupler_at", "exit_end")]
     o.scale_multipoles = 1 if e.scale_multipoles else 0
     for n in _DBLS:
         if n in e.values:

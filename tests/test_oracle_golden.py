@@ -82,6 +82,11 @@ ELEMENTS = {
     "MULTIPOLE1": ("multipole", {"x_offset": 0.05}, {"a_pole": {1: 1.0, 3: 4.5}, "b_pole": {1: PI / 4, 3: 0.31 * PI}}),
     "RFCAVITY1": ("rfcavity", {"l": 4.5, "rf_frequency": 500e6, "voltage": 1e5, "phi0": 0.1, "x_offset": 0.05,
                                "y_pitch": 0.001, "tilt": 0.1}, {"num_steps": 10}),
+    # cavity_type = traveling_wave (tracking_method_test.bmad:71-72) changes
+    # nothing in bmad_standard rfcavity tracking; the coupler kick does
+    "RFCAVITY2": ("rfcavity", {"l": 4.5, "rf_frequency": 500e6, "voltage": 1e5, "phi0": 0.1, "x_offset": 0.05,
+                               "y_pitch": 0.001, "tilt": 0.1, "coupler_strength": 0.1},
+                  {"num_steps": 10, "coupler_at": "both_ends"}),
     "RFCAVITY3": ("rfcavity", {"rf_frequency": 500e6, "voltage": 1e5, "phi0": 0.1, "x_offset": 0.05,
                                "y_pitch": 0.001, "tilt": 0.1}, {"num_steps": 10, "a_pole": {2: 0.02}}),
 }
