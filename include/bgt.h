@@ -205,12 +205,15 @@ int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, int32_t* state
 
 /*
  * Dynamic-aperture scan on a polar grid, one launch for all variants:
- * for each variant v, angle a (n_angle in [angle_min, angle_max]), radius r
- * (n_radius from 0 to r_max), and momentum offset d (n_delta values in
- * deltas[]), the particle starts at ref_orbit[v] (6 coords, the closed orbit
- * of variant v at the start, with pz set to deltas[d] ... plus eta*pz when
- * the caller includes it) + (r cos a, 0, r sin a * y_scale, 0, 0, 0) and is
- * tracked n_turns turns.  da_radius[((v * n_delta) + d) * n_angle + a] receives
+ * for each variant v, momentum offset d (n_delta of them), angle a (n_angle
+ * in [angle_min, angle_max]) and radius r (n_radius from 0 to r_max), the
+ * particle starts at ref_orbit[(v * n_delta + d) * 6 + c] -- the reference
+ * orbit of variant v at the d-th momentum offset: its closed orbit with pz
+ * set to that offset, plus eta*pz when the caller includes it, as
+ * dynamic_aperture_mod.f90:132-140 forms it -- plus (r cos a, 0,
+ * r sin a * y_scale, 0, 0, 0), and is tracked n_turns turns.  The offsets
+ * themselves are part of ref_orbit: deltas[] (n_delta values, may be NULL)
+ * is not read.  da_radius[((v * n_delta) + d) * n_angle + a] receives
  * the largest grid radius below the first lost one along that ray (the
  * lower bracket x0 of dynamic_aperture_point, dynamic_aperture_mod.f90:
  * 335-388); survive_turns (optional, may be NULL) receives, per particle in
