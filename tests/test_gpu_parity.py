@@ -179,6 +179,39 @@ def test_compaction_and_tiles_do_not_change_results():
         assert np.array_equal(o.vec6, outs[0].vec6)
 
 
+def test_ragged_sizes_empty_calls_and_lost_input():
+    """Particle counts that fill no tile (1, 33, 257) in every table
+    placement, a nonzero start turn (loss turns are absolute), the empty
+    call, zero turns, and particles already lost on input (left as they
+    are)."""
+    lat = rings.fodo_ring(apertures=True)
+    v_all = rings.gaussian_beam(rings.BeamSpec(300, 4e-6, 2e-6, 3e-3, 2e-3, seed=79))
+    for mode in (0, 2, 3):
+        tr = Tracker(lat, tuning=dict(threads_per_block=128, blocks_per_sm=4, table_mode=mode))
+        for n in (1, 33, 257):
+            v0 = v_all[:, :n].copy()
+            b = tr.make_bunch(v0.copy())
+            tr.track_turns(b, 20, turn0=5)
+            ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), 20, variant="cr")
+            oit = np.where(ost != L.ALIVE, oit + 5, oit)
+            assert_bitwise(b, ov, ob, ost, oie, oit, f"n={n} table_mode={mode}")
+    tr = Tracker(lat)
+    launches = tr.launch_count
+    empty = tr.make_bunch(np.zeros((6, 0)))
+    tr.track_turns(empty, 5)
+    b = tr.make_bunch(v_all.copy())
+    tr.track_turns(b, 0)
+    assert tr.launch_count == launches and np.array_equal(b.vec6, v_all)
+    b.state[::3] = L.LOST_NEG_X
+    b.ix_ele_lost[::3] = 7
+    b.ix_turn_lost[::3] = 2
+    before = b.vec6[:, ::3].copy()
+    tr.track_turns(b, 10, turn0=3)
+    assert np.array_equal(b.vec6[:, ::3], before)
+    assert np.all(b.state[::3] == L.LOST_NEG_X) and np.all(b.ix_ele_lost[::3] == 7)
+    assert np.all(b.ix_turn_lost[::3] == 2)
+
+
 def test_variants_batched():
     lats = rings.error_variants(4, seed=5)
     tr = Tracker(lats)
