@@ -8,6 +8,7 @@ Sources (relative to the reference root):
   regression_tests/tracking_method_test/output.correct  ("<ELE>: Bmad_Standard" rows)
   regression_tests/fringe_test/output.correct           (Hwang edge kick deltas)
   regression_tests/aperture_test/output.correct         (aperture states, unstable factors)
+  regression_tests/multipole_test/output.correct        ("MULT-<tilt><kicks>-<ELE>" rows: multipole_ele_to_ab)
 """
 import json
 import re
@@ -51,8 +52,15 @@ def main(ref: Path):
         if p and re.match(r"(EC|RC)_[SU]_", p[0]):
             ap[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3]], "text": p[3]}
     out["aperture"] = ap
+    mp = {}
+    for line in (ref / "regression_tests/multipole_test/output.correct").read_text().splitlines():
+        p = parse_line(line)
+        if p and re.match(r"MULT-[12][12]-(QQ|BB|MM|EE)$", p[0]):
+            mp[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3][:6]], "ix": int(p[3][6]), "text": p[3][:6]}
+    out["multipole"] = mp
     (HERE / "reference_golden.json").write_text(json.dumps(out, indent=1, sort_keys=True))
-    print(f"tracking_method rows: {len(rows)}, fringe rows: {len(fr)}, aperture rows: {len(ap)}")
+    print(f"tracking_method rows: {len(rows)}, fringe rows: {len(fr)}, aperture rows: {len(ap)}, "
+          f"multipole rows: {len(mp)}")
 
 
 if __name__ == "__main__":
