@@ -1058,9 +1058,11 @@ static void bend_offset_position(const bgo_ele* ele, int set, int drift_to, doub
 
 /* offset_particle, bmad/code/offset_particle.f90:66-530, forward tracking.
  * s_pos_mode: 0 = normal (drift to the edge), 1 = s_pos given (no drift),
- * with s_pos the lab (set) / body (unset) position. */
-static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int set_tilt, int set_hvkicks,
-                            int s_pos_mode, double s_pos, const bgo_param* param) {
+ * with s_pos the lab (set) / body (unset) position.  s_out (may be NULL):
+ * the edge drifted to, or the body (set) / lab (unset) position (:334-336,
+ * :486-492). */
+static void offset_particle_s(const bgo_ele* ele, int set, bgo_coord* orbit, int set_tilt, int set_hvkicks,
+                              int s_pos_mode, double s_pos, const bgo_param* param, double* s_out) {
   double length = ele->l;
   double L_half = 0.5 * length;
   int has_orient = !(ele->key == BGO_MULTIPOLE && 0); /* all path elements carry orientation attributes */
@@ -1122,6 +1124,7 @@ static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int s
     }
     double ds = s_target - s_body;
     if (fabs(ds) > 1e-14 && drift_to != 0 && orbit->state == BGO_ALIVE) track_a_drift(orbit, ds, 0, param);
+    if (s_out) *s_out = drift_to != 0 ? s_target : s_body;
     if (set_hv1) {
       orbit->vec[1] = orbit->vec[1] + 0.5 * charge_dir * ele->hkick;
       orbit->vec[3] = orbit->vec[3] + 0.5 * charge_dir * ele->vkick;
@@ -1189,7 +1192,21 @@ static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int s
     }
     double ds = s_target - s_lab;
     if (fabs(ds) > 1e-14 && drift_to != 0 && orbit->state == BGO_ALIVE) track_a_drift(orbit, ds, 0, param);
+    if (s_out) *s_out = drift_to != 0 ? s_target : s_lab;
   }
+}
+
+static void offset_particle(const bgo_ele* ele, int set, bgo_coord* orbit, int set_tilt, int set_hvkicks,
+                            int s_pos_mode, double s_pos, const bgo_param* param) {
+  offset_particle_s(ele, set, orbit, set_tilt, set_hvkicks, s_pos_mode, s_pos, param, NULL);
+}
+
+/* offset_particle(ele, set$ or unset$, orbit) with its default tilt and hv
+ * kicks; drift_to_edge = no$ with s_pos when s_pos_mode is 1 (the form the
+ * reference's coord_test exercises).  Test entry point. */
+void bgo_offset_particle(const bgo_ele* ele, int set, bgo_coord* orb, int s_pos_mode, double s_pos,
+                         const bgo_param* param, double* s_out) {
+  offset_particle_s(ele, set, orb, 1, 1, s_pos_mode, s_pos, param, s_out);
 }
 
 /* ------------------------------------------------------------------ */

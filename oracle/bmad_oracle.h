@@ -139,6 +139,8 @@ void bgo_track1(bgo_coord* orb, const bgo_ele* ele, bgo_param* param);
 int bgo_orbit_too_large(bgo_coord* orb, bgo_param* param);
 void bgo_check_aperture_limit(bgo_coord* orb, const bgo_ele* ele, int at_exit, bgo_param* param);
 void bgo_hwang_bend_edge_kick(const bgo_ele* ele, int entering, bgo_coord* orb, const bgo_param* param);
+void bgo_offset_particle(const bgo_ele* ele, int set, bgo_coord* orb, int s_pos_mode, double s_pos,
+                         const bgo_param* param, double* s_out);
 
 /* ---- lattice / multi-turn drivers ----
  * Coordinates are SoA: x[n], px[n], ... (six arrays packed as vec6[6*n], index c*n+i)

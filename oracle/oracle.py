@@ -75,6 +75,8 @@ def _bind(lib):
     lib.bgo_check_aperture_limit.argtypes = [C.POINTER(Coord), C.POINTER(Ele), C.c_int, C.POINTER(Param)]
     lib.bgo_hwang_bend_edge_kick.argtypes = [C.POINTER(Ele), C.c_int, C.POINTER(Coord), C.POINTER(Param)]
     lib.bgo_orbit_too_large.argtypes = [C.POINTER(Coord), C.POINTER(Param)]
+    lib.bgo_offset_particle.argtypes = [C.POINTER(Ele), C.c_int, C.POINTER(Coord), C.c_int, C.c_double,
+                                        C.POINTER(Param), C.POINTER(C.c_double)]
     lib.bgo_track_turns.argtypes = [C.POINTER(Ele), C.c_int, C.POINTER(Param), C.c_double, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int), C.c_long, C.c_int, C.c_int, C.c_int, C.c_int]

@@ -9,6 +9,8 @@ Sources (relative to the reference root):
   regression_tests/fringe_test/output.correct           (Hwang edge kick deltas)
   regression_tests/aperture_test/output.correct         (aperture states, unstable factors)
   regression_tests/multipole_test/output.correct        ("MULT-<tilt><kicks>-<ELE>" rows: multipole_ele_to_ab)
+  regression_tests/coord_test/output.correct            (offset_particle set / unset, forward rows of the
+                                                         misaligned solenoid and bends)
 """
 import json
 import re
@@ -58,9 +60,15 @@ def main(ref: Path):
         if p and re.match(r"MULT-[12][12]-(QQ|BB|MM|EE)$", p[0]):
             mp[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3][:6]], "ix": int(p[3][6]), "text": p[3][:6]}
     out["multipole"] = mp
+    co = {}
+    for line in (ref / "regression_tests/coord_test/output.correct").read_text().splitlines():
+        p = parse_line(line)
+        if p and re.match(r"(Q1|B0|B1|B2):O:1:D:1:.*-orb$", p[0]):
+            co[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3]], "text": p[3]}
+    out["coord"] = co
     (HERE / "reference_golden.json").write_text(json.dumps(out, indent=1, sort_keys=True))
     print(f"tracking_method rows: {len(rows)}, fringe rows: {len(fr)}, aperture rows: {len(ap)}, "
-          f"multipole rows: {len(mp)}")
+          f"multipole rows: {len(mp)}, coord rows: {len(co)}")
 
 
 if __name__ == "__main__":
