@@ -161,8 +161,9 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "fodo64 ring + apertures, config-1 beam (sampled)", "particles": n_sample,
-                       "turns_per_step": t_sample, "parallelism": f"openmp x{threads}"},
+            "config": {"workload": "fodo64 ring (770 elements) + apertures, config-1 beam",
+                       "particles_per_step_sample": n_sample, "turns_per_step": t_sample,
+                       "parallelism": f"openmp x{threads}"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
