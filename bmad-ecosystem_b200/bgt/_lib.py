@@ -31,7 +31,7 @@ class BgtElement(C.Structure):
             "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",
             "x1_limit", "x2_limit", "y1_limit", "y2_limit")] + [
         (n, C.c_double * N_POLE) for n in ("an", "bn", "an_elec", "bn_elec", "knl", "tn")] + [
-        ("coupler_angle", C.c_double), ("coupler_phase", C.c_double)]
+        ("coupler_angle", C.c_double), ("coupler_phase", C.c_double), ("fq1", C.c_double), ("fq2", C.c_double)]
 
 
 class BgtSpecies(C.Structure):
@@ -119,6 +119,8 @@ def to_bgt_element(e: L.Element) -> BgtElement:
     b.coupler_at = L.ENDS[e.coupler_at]
     b.coupler_angle = e.v("coupler_angle")
     b.coupler_phase = e.v("coupler_phase")
+    b.fq1 = e.v("fq1")
+    b.fq2 = e.v("fq2")
     for n in ("l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
               "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset",
               "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",

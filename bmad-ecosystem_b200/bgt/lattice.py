@@ -60,7 +60,7 @@ _VALUE_NAMES = [
     "l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
     "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset", "y_offset",
     "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick", "x1_limit",
-    "x2_limit", "y1_limit", "y2_limit", "r0_mag", "r0_elec", "coupler_angle", "coupler_phase",
+    "x2_limit", "y1_limit", "y2_limit", "r0_mag", "r0_elec", "coupler_angle", "coupler_phase", "fq1", "fq2",
 ]
 
 

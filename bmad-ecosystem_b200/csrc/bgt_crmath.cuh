@@ -1,4 +1,4 @@
-// bgt_crmath.cuh -- correctly rounded FP64 sin, cos, asin, atan2 for the
+// bgt_crmath.cuh -- correctly rounded FP64 sin, cos, sinh, cosh, exp, asin, atan2 for the
 // tracker's device code (and, compiled for the host, for testing).
 //
 // Why: the exact sector-bend map (track_a_bend.f90:163-209) cancels
@@ -15,7 +15,8 @@
 //               same double, that double is the correctly rounded result.
 //   slow path   full double-double Taylor evaluation after Cody-Waite
 //               argument reduction (sin/cos), argument halving (atan) or
-//               the half-angle identity (asin): error ~2^-100, then round.
+//               the half-angle identity (asin), on the argument itself for
+//               sinh/cosh/exp (|x| <= 2): error ~2^-100, then round.
 // Arguments beyond the documented ranges (|x| >= 2^19 for sin/cos,
 // non-finite values, extreme atan2 exponents) use the CUDA / C library
 // function.
@@ -349,6 +350,39 @@ BGT_HD double cosh(double x) {
     if (round_test(acc, err, &out)) return out;
   }
   dd r = dd_cosh_kernel(x);
+  return r.hi + r.lo;
+}
+
+// ---- exp (|x| <= 2; larger arguments use the library) ----
+//
+// Light path, 2^-54 <= |x| <= 2^-4: e^x = (1 + x) + x^2 P(x) with
+// P(x) = 1/2 + x/6 + ... + x^13/15! in plain double (Horner); 1 + x is exact
+// as a double-double (two_sum), |x^2 P| <= 0.52 x^2 <= 2^-8.9.  Relative
+// error of c = x^2 P: the square (u), P (< 1.2u: its leading 1/2 is exact
+// and the next term is below x/6), the product (u) -> < 4u < 2^-50; the
+// omitted terms are < x^16/16! < 2^-108; the add into 1 + x < 2^-105.
+// Below 2^-54 the correctly rounded value is 1.  Accurate path: the Taylor
+// series to x^40/40! in double-double (Horner), error < 2^-99 relative.
+
+BGT_HD_NOINLINE dd dd_exp_kernel(double x) {
+  dd acc = dd_c(EXP_C[40]);
+  for (int k = 39; k >= 0; k--) acc = dd_add(dd_mul_d(acc, x), dd_c(EXP_C[k]));
+  return acc;
+}
+
+BGT_HD double exp(double x) {
+  double a = fabs(x);
+  if (!(a <= 2.0)) return ::exp(x);
+  if (a < 0x1p-54) return 1.0;
+  if (a <= 0x1p-4) {
+    double p = EXP_C[15][0];
+    for (int k = 14; k >= 2; k--) p = p * x + EXP_C[k][0];
+    double c = (x * x) * p;
+    dd acc = dd_add_d(two_sum(1.0, x), c);
+    double out;
+    if (round_test(acc, fabs(c) * 0x1p-50 + 0x1p-104, &out)) return out;
+  }
+  dd r = dd_exp_kernel(x);
   return r.hi + r.lo;
 }
 

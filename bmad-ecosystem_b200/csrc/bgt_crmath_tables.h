@@ -186,6 +186,99 @@ static const double COSH_C_host[17][2] = {
 #define COSH_C COSH_C_host
 #endif
 #ifdef __CUDACC__
+__constant__ double EXP_C_dev[41][2] = {
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p-1, 0.0},
+    {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+    {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65},
+    {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+    {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76},
+    {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80},
+    {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83},
+    {0x1.6124613a86d09p-33, 0x1.f28e0cc748ebep-87},
+    {0x1.93974a8c07c9dp-37, 0x1.05d6f8a2efd1fp-92},
+    {0x1.ae7f3e733b81fp-41, 0x1.1d8656b0ee8cbp-97},
+    {0x1.ae7f3e733b81fp-45, 0x1.1d8656b0ee8cbp-101},
+    {0x1.952c77030ad4ap-49, 0x1.ac981465ddc6cp-103},
+    {0x1.6827863b97d97p-53, 0x1.eec01221a8b0bp-107},
+    {0x1.2f49b46814157p-57, 0x1.2650f61dbdcb4p-112},
+    {0x1.e542ba4020225p-62, 0x1.ea72b4afe3c2fp-120},
+    {0x1.71b8ef6dcf572p-66, -0x1.d043ae40c4647p-120},
+    {0x1.0ce396db7f853p-70, -0x1.aebcdbd20331cp-124},
+    {0x1.761b41316381ap-75, -0x1.3423c7d91404fp-130},
+    {0x1.f2cf01972f578p-80, -0x1.9ada5fcc1ab14p-135},
+    {0x1.3f3ccdd165fa9p-84, -0x1.58ddadf344487p-139},
+    {0x1.88e85fc6a4e5ap-89, -0x1.71c37ebd16540p-143},
+    {0x1.d1ab1c2dccea3p-94, 0x1.054d0c78aea14p-149},
+    {0x1.0a18a2635085dp-98, 0x1.b9e2e28e1aa54p-153},
+    {0x1.259f98b4358adp-103, 0x1.eaf8c39dd9bc5p-157},
+    {0x1.3932c5047d60ep-108, 0x1.832b7b530a627p-162},
+    {0x1.434d2e783f5bcp-113, 0x1.0b87b91be9affp-167},
+    {0x1.434d2e783f5bcp-118, 0x1.0b87b91be9affp-172},
+    {0x1.3981254dd0d52p-123, -0x1.2b1f4c8015a2fp-177},
+    {0x1.2710231c0fd7ap-128, 0x1.3f8a2b4af9d6bp-184},
+    {0x1.0dc59c716d91fp-133, 0x1.419e3fad3f031p-188},
+    {0x1.df983290c2ca9p-139, 0x1.5835c6895393bp-194},
+    {0x1.9ec8d1c94e85bp-144, -0x1.670e9d4784ec6p-201},
+    {0x1.5d4acb9c0c3abp-149, -0x1.6ec2c8f5b13b2p-205},
+    {0x1.1e99449a4bacep-154, -0x1.fefbb89514b3cp-210},
+    {0x1.ca8ed42a12ae3p-160, 0x1.a07244abad2abp-224},
+};
+#endif
+static const double EXP_C_host[41][2] = {
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p+0, 0.0},
+    {0x1.0000000000000p-1, 0.0},
+    {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+    {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65},
+    {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+    {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76},
+    {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80},
+    {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83},
+    {0x1.6124613a86d09p-33, 0x1.f28e0cc748ebep-87},
+    {0x1.93974a8c07c9dp-37, 0x1.05d6f8a2efd1fp-92},
+    {0x1.ae7f3e733b81fp-41, 0x1.1d8656b0ee8cbp-97},
+    {0x1.ae7f3e733b81fp-45, 0x1.1d8656b0ee8cbp-101},
+    {0x1.952c77030ad4ap-49, 0x1.ac981465ddc6cp-103},
+    {0x1.6827863b97d97p-53, 0x1.eec01221a8b0bp-107},
+    {0x1.2f49b46814157p-57, 0x1.2650f61dbdcb4p-112},
+    {0x1.e542ba4020225p-62, 0x1.ea72b4afe3c2fp-120},
+    {0x1.71b8ef6dcf572p-66, -0x1.d043ae40c4647p-120},
+    {0x1.0ce396db7f853p-70, -0x1.aebcdbd20331cp-124},
+    {0x1.761b41316381ap-75, -0x1.3423c7d91404fp-130},
+    {0x1.f2cf01972f578p-80, -0x1.9ada5fcc1ab14p-135},
+    {0x1.3f3ccdd165fa9p-84, -0x1.58ddadf344487p-139},
+    {0x1.88e85fc6a4e5ap-89, -0x1.71c37ebd16540p-143},
+    {0x1.d1ab1c2dccea3p-94, 0x1.054d0c78aea14p-149},
+    {0x1.0a18a2635085dp-98, 0x1.b9e2e28e1aa54p-153},
+    {0x1.259f98b4358adp-103, 0x1.eaf8c39dd9bc5p-157},
+    {0x1.3932c5047d60ep-108, 0x1.832b7b530a627p-162},
+    {0x1.434d2e783f5bcp-113, 0x1.0b87b91be9affp-167},
+    {0x1.434d2e783f5bcp-118, 0x1.0b87b91be9affp-172},
+    {0x1.3981254dd0d52p-123, -0x1.2b1f4c8015a2fp-177},
+    {0x1.2710231c0fd7ap-128, 0x1.3f8a2b4af9d6bp-184},
+    {0x1.0dc59c716d91fp-133, 0x1.419e3fad3f031p-188},
+    {0x1.df983290c2ca9p-139, 0x1.5835c6895393bp-194},
+    {0x1.9ec8d1c94e85bp-144, -0x1.670e9d4784ec6p-201},
+    {0x1.5d4acb9c0c3abp-149, -0x1.6ec2c8f5b13b2p-205},
+    {0x1.1e99449a4bacep-154, -0x1.fefbb89514b3cp-210},
+    {0x1.ca8ed42a12ae3p-160, 0x1.a07244abad2abp-224},
+};
+#ifdef __CUDA_ARCH__
+#define EXP_C EXP_C_dev
+#else
+#define EXP_C EXP_C_host
+#endif
+#ifdef __CUDACC__
 __constant__ double ASIN_C_dev[40][2] = {
     {0x1.0000000000000p+0, 0.0},
     {0x1.5555555555555p-3, 0x1.5555555555555p-57},

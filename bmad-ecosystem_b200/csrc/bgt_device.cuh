@@ -616,6 +616,26 @@ __device__ __forceinline__ void hard_multipole_edge_kick(Part& p, double bp, boo
   p.z = p.z + (p.px * fx + p.py * fy) / rel_p;
 }
 
+// soft_quadrupole_edge_kick, bmad/modules/fringe_mod.f90:555-660 (tracking
+// part, charge_dir = 1): s = (k1, fq1, fq2); the exponential of the
+// particle-dependent f1 is correctly rounded, as the C library gives it.
+__device__ __forceinline__ void soft_quad_edge_kick(Part& p, const double* s, bool first_edge) {
+  const double rel_p = 1 + p.pz;
+  const double k1_rel = 1.0 * s[0] / rel_p;
+  double f1 = k1_rel * s[1];
+  const double f2 = k1_rel * s[2];
+  if (f1 == 0 && f2 == 0) return;
+  if (!first_edge) f1 = -f1;
+  const double ef1 = cr::exp(f1);
+  const double x = p.x, px = p.px, y = p.y, py = p.py;
+  const double vx = px / rel_p, vy = py / rel_p;
+  p.z = p.z - (f1 * x + f2 * (1 + f1 / 2) * vx / ef1) * vx + (f1 * y + f2 * (1 - f1 / 2) * vy * ef1) * vy;
+  p.x = x * ef1 + vx * f2;
+  p.px = px / ef1;
+  p.y = y / ef1 - vy * f2;
+  p.py = py * ef1;
+}
+
 // ---------------------------------------------------------------------------
 // Hwang hard-edge bend fringe, bmad/modules/fringe_mod.f90:240-418 (td = +1)
 template <bool ENTERING>

@@ -81,11 +81,14 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
   const double* ae = an + 2 * (ix + 1);
   const double* be = ae + (ixe + 1);
   const double* hard = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);
+  const double* soft = hard + ((fl & F_HARD_EDGE) ? 1 : 0);
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
   if (RARE && (fl & F_FRINGE_INFO)) {
-    // apply_element_edge_kick.f90:160-176, first edge: magnetic, then electric
+    // apply_element_edge_kick.f90:160-176, first edge: magnetic (hard, then
+    // soft), then electric
     if (fl & F_EDGE_IN) {
       if (fl & F_HARD_EDGE) hard_multipole_edge_kick<1>(p, hard[0], true);
+      if (fl & F_SOFT_EDGE) soft_quad_edge_kick(p, soft, true);
       if (fl & F_ELEC_EDGE) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
     }
     if (p.state != ALIVE) return;
@@ -132,9 +135,10 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
     if (RARE && ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, (i == n_step) ? q[Q_STEP] / 2 : q[Q_STEP], G);
   }
   if (RARE && (fl & F_FRINGE_INFO)) {
-    // second edge: electric, then magnetic
+    // second edge: electric, then magnetic (soft, then hard)
     if (fl & F_EDGE_OUT) {
       if (fl & F_ELEC_EDGE) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+      if (fl & F_SOFT_EDGE) soft_quad_edge_kick(p, soft, false);
       if (fl & F_HARD_EDGE) hard_multipole_edge_kick<1>(p, hard[0], false);
     }
     if (p.state != ALIVE) return;

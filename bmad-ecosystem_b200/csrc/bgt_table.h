@@ -66,6 +66,9 @@ enum Flag : int32_t {
   // rfcavity coupler kick at the entrance / exit (rf_coupler_kick.f90)
   F_COUPLER_IN = 1 << 22,
   F_COUPLER_OUT = 1 << 23,
+  // quadrupole soft-edge fringe (fringe_type full or soft_edge_only with
+  // fq1 or fq2 nonzero): k1, fq1, fq2 follow the hard-edge strength
+  F_SOFT_EDGE = 1 << 24,
 };
 
 struct RecHdr {

@@ -715,13 +715,22 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       if (e.l != 0) flags |= F_ELEC_EDGE;
     }
     // hard_multipole_edge_kick (fringe_mod.f90:691-864) for quadrupoles and
-    // sextupoles; soft_quadrupole_edge_kick is zero for fq1 = fq2 = 0 (the
-    // defaults, the only values this table carries)
+    // sextupoles
     if ((e.fringe_type == BGT_FRINGE_FULL || e.fringe_type == BGT_FRINGE_HARD_EDGE_ONLY) &&
         (key == BGT_QUADRUPOLE || key == BGT_SEXTUPOLE)) {
       flags |= F_HARD_EDGE;
       double* q = B.ptr_after_push(1);
       q[0] = (key == BGT_QUADRUPOLE) ? e.k1 : e.k2;
+    }
+    // soft_quadrupole_edge_kick (fringe_mod.f90:555-660): nothing unless fq1
+    // or fq2 is nonzero
+    if ((e.fringe_type == BGT_FRINGE_FULL || e.fringe_type == BGT_FRINGE_SOFT_EDGE_ONLY) &&
+        key == BGT_QUADRUPOLE && (e.fq1 != 0 || e.fq2 != 0)) {
+      flags |= F_SOFT_EDGE;
+      double* q = B.ptr_after_push(3);
+      q[0] = e.k1;
+      q[1] = e.fq1;
+      q[2] = e.fq2;
     }
   }
   h.flags = flags;

@@ -4,7 +4,8 @@ literals.
 
     python gen_crmath_tables.py > bgt_crmath_tables.h
 
-Coefficients are exact rationals (Taylor series of sin, cos, asin, atan);
+Coefficients are exact rationals (Taylor series of sin, cos, sinh, cosh, exp,
+asin, atan);
 pi/2 and pi are taken to 200 bits from a Machin-formula evaluation.
 """
 from fractions import Fraction as F
@@ -95,6 +96,8 @@ def main():
     # sinh: 1 / (2k+1)!, cosh: 1 / (2k)!,  k = 0..16
     arr("SINH_C", [F(1, factorial(2 * k + 1)) for k in range(17)])
     arr("COSH_C", [F(1, factorial(2 * k)) for k in range(17)])
+    # exp: 1 / k!,  k = 0..40
+    arr("EXP_C", [F(1, factorial(k)) for k in range(41)])
     # asin: (2k)! / (4^k (k!)^2 (2k+1)),  k = 0..39
     arr("ASIN_C", [F(factorial(2 * k), 4 ** k * factorial(k) ** 2 * (2 * k + 1)) for k in range(40)])
     # atan: (-1)^k / (2k+1),  k = 0..39

@@ -132,6 +132,7 @@ typedef struct bgt_element {
   double an_elec[BGT_N_POLE], bn_elec[BGT_N_POLE];
   double knl[BGT_N_POLE], tn[BGT_N_POLE];
   double coupler_angle, coupler_phase; /* rfcavity coupler (with coupler_strength) */
+  double fq1, fq2;                     /* quadrupole soft-edge fringe integrals */
 } bgt_element;
 
 /* Tracked species (lat%param%particle) and bmad_com switches. */

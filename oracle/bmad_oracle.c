@@ -65,6 +65,7 @@ static double P_ASIN(double x) { return (double)asinq((__float128)x); }
 static double P_ATAN2(double y, double x) { return (double)atan2q((__float128)y, (__float128)x); }
 static double P_SINH(double x) { return (double)sinhq((__float128)x); }
 static double P_COSH(double x) { return (double)coshq((__float128)x); }
+static double P_EXP(double x) { return (double)expq((__float128)x); }
 #else
 #define P_SIN sin
 #define P_COS cos
@@ -72,6 +73,7 @@ static double P_COSH(double x) { return (double)coshq((__float128)x); }
 #define P_ATAN2 atan2
 #define P_SINH sinh
 #define P_COSH cosh
+#define P_EXP exp
 #endif
 
 /* x**m for integer m, as gfortran evaluates it (repeated squaring,
@@ -1557,6 +1559,30 @@ static void hard_multipole_edge_kick(const bgo_ele* ele, int first_edge, bgo_coo
 
 /* apply_element_edge_kick, bmad/low_level/apply_element_edge_kick.f90:37-278
  * for the bmad_standard field_calc case.  Returns -1 for unsupported forms. */
+/* soft_quadrupole_edge_kick, bmad/modules/fringe_mod.f90:555-660 (tracking
+ * part): the soft-edge fringe of a quadrupole with the fringe integrals
+ * fq1, fq2; charge_dir = 1 (forward tracking of the reference species). */
+static void soft_quadrupole_edge_kick(const bgo_ele* ele, int first_edge, bgo_coord* orb) {
+  if (ele->fringe_type != BGO_FRINGE_SOFT_EDGE_ONLY && ele->fringe_type != BGO_FRINGE_FULL) return;
+  double rel_p = 1 + orb->vec[5];
+  double k1_rel = 1.0 * ele->k1 / rel_p;
+  double f1 = k1_rel * ele->fq1;
+  double f2 = k1_rel * ele->fq2;
+  if (f1 == 0 && f2 == 0) return;
+  if (!first_edge) f1 = -f1;
+  double ef1 = P_EXP(f1);
+  double x = orb->vec[0], px = orb->vec[1], y = orb->vec[2], py = orb->vec[3];
+  double vx = px / rel_p, vy = py / rel_p;
+  orb->vec[4] = orb->vec[4] - (f1 * x + f2 * (1 + f1 / 2) * vx / ef1) * vx +
+                (f1 * y + f2 * (1 - f1 / 2) * vy * ef1) * vy;
+  orb->vec[0] = x * ef1 + vx * f2;
+  orb->vec[1] = px / ef1;
+  orb->vec[2] = y / ef1 - vy * f2;
+  orb->vec[3] = py * ef1;
+  LM(1);
+  FL(40);
+}
+
 static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first_edge, const bgo_param* param,
                                    const double* ae, const double* be, int ix_elec_max) {
   int physical_end = first_edge ? BGO_ENTRANCE_END : BGO_EXIT_END;
@@ -1567,14 +1593,20 @@ static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first
   if (!first_edge) electric_longitudinal_fringe(orb, ele, ae, be, ix_elec_max, at_sign, param);
   switch (ele->key) {
     case BGO_QUADRUPOLE:
-    case BGO_SEXTUPOLE:
+    case BGO_SEXTUPOLE: {
       /* apply_element_edge_kick.f90:173-186: quadrupole entrance hard then
-       * soft, exit soft then hard; sextupole hard only.  The soft
-       * quadrupole edge (soft_quadrupole_edge_kick, fringe_mod.f90:555-660)
-       * is zero for fq1 = fq2 = 0, the defaults, which are assumed here. */
-      if (ele->fringe_type == BGO_FRINGE_FULL || ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY)
-        hard_multipole_edge_kick(ele, first_edge, orb);
+       * soft, exit soft then hard; sextupole hard only. */
+      int hard = ele->fringe_type == BGO_FRINGE_FULL || ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY;
+      int soft = ele->key == BGO_QUADRUPOLE;
+      if (first_edge) {
+        if (hard) hard_multipole_edge_kick(ele, first_edge, orb);
+        if (soft) soft_quadrupole_edge_kick(ele, first_edge, orb);
+      } else {
+        if (soft) soft_quadrupole_edge_kick(ele, first_edge, orb);
+        if (hard) hard_multipole_edge_kick(ele, first_edge, orb);
+      }
       break;
+    }
     case BGO_SBEND:
       /* bend_edge_kick, fringe_mod.f90:39-127: fringe_here, hard multipole edge
        * (only for fringe_type full: not restated), then Hwang. */

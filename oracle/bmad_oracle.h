@@ -120,6 +120,7 @@ typedef struct bgo_ele {
   double z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center;
   double r0_mag, r0_elec;
   double coupler_strength, coupler_angle, coupler_phase;
+  double fq1, fq2;
   /* For BGO_MULTIPOLE: a_pole = knl, b_pole = tn, ksl_pole = ksl (pointer_to_ele_multipole). */
   double a_pole[BGO_N_POLE], b_pole[BGO_N_POLE], ksl_pole[BGO_N_POLE];
   double a_pole_elec[BGO_N_POLE], b_pole_elec[BGO_N_POLE];

@@ -47,7 +47,7 @@ _DBLS = ["l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", 
          "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick", "x1_limit", "x2_limit", "y1_limit",
          "y2_limit", "px_aperture_width2", "px_aperture_center", "py_aperture_width2", "py_aperture_center",
          "z_aperture_width2", "z_aperture_center", "pz_aperture_width2", "pz_aperture_center", "r0_mag", "r0_elec",
-         "coupler_strength", "coupler_angle", "coupler_phase"]
+         "coupler_strength", "coupler_angle", "coupler_phase", "fq1", "fq2"]
 
 
 class Ele(C.Structure):

@@ -1,4 +1,4 @@
-// Host check of the device's correctly rounded sin/cos/sinh/cosh/asin/atan2
+// Host check of the device's correctly rounded sin/cos/sinh/cosh/exp/asin/atan2
 // (bmad-ecosystem_b200/csrc/bgt_crmath.cuh, compiled here for the CPU)
 // against libquadmath evaluated in binary128 and rounded to double.
 //
@@ -41,6 +41,7 @@ static double cr_eval(const char* fn, double x, double y) {
   if (!strcmp(fn, "sinh")) return bgt::cr::sinh(x);
   if (!strcmp(fn, "cosh")) return bgt::cr::cosh(x);
   if (!strcmp(fn, "asin")) return bgt::cr::asin(x);
+  if (!strcmp(fn, "exp")) return bgt::cr::exp(x);
   return bgt::cr::atan2(y, x);
 }
 static double q_eval(const char* fn, double x, double y) {
@@ -50,6 +51,7 @@ static double q_eval(const char* fn, double x, double y) {
   else if (!strcmp(fn, "sinh")) q = sinhq(x);
   else if (!strcmp(fn, "cosh")) q = coshq(x);
   else if (!strcmp(fn, "asin")) q = asinq(x);
+  else if (!strcmp(fn, "exp")) q = expq(x);
   else q = atan2q(y, x);
   return (double)q;
 }
@@ -63,11 +65,13 @@ int main(int argc, char** argv) {
       {"sin", 0x1p-30, 0x1p-4, 1}, {"sin", -0.0625, 0.0625, 0}, {"sin", 0.0155, 0.0175, 0},
       {"cos", 0x1p-30, 0x1p-4, 1}, {"cos", -0.0625, 0.0625, 0},
       {"sinh", 0x1p-30, 0x1p-4, 1}, {"cosh", 0x1p-30, 0x1p-4, 1},
+      {"exp", 0x1p-60, 0x1p-4, 1}, {"exp", -0.0625, 0.0625, 0},
       {"asin", 0x1p-30, 0x1p-4, 1}, {"asin", -2e-3, 2e-3, 0},
       {"atan2", 0x1p-30, 0x1p-4, 1}, {"atan2", -0.0625, 0.0625, 0},
       // double-double fast paths and the slow paths behind them
       {"sin", -0.78, 0.78, 0}, {"sin", -30.0, 30.0, 0}, {"cos", -0.78, 0.78, 0}, {"cos", -30.0, 30.0, 0},
-      {"sinh", -2.0, 2.0, 0}, {"cosh", -2.0, 2.0, 0}, {"asin", -1.0, 1.0, 0}, {"atan2", -4.0, 4.0, 0},
+      {"sinh", -2.0, 2.0, 0}, {"cosh", -2.0, 2.0, 0}, {"exp", -2.0, 2.0, 0}, {"asin", -1.0, 1.0, 0},
+      {"atan2", -4.0, 4.0, 0},
   };
   long total_bad = 0;
   for (const Range& r : rs) {

@@ -83,9 +83,9 @@ def rare_zoo_lattice() -> L.Lattice:
     """Element forms that only the device's RARE kernels handle: misaligned
     bends (offset_particle's bend geometry, with g, ref_tilt or roll), the
     straight geometry of a misaligned g = 0 bend, electric multipoles in bends
-    and quadrupoles, the hard-edge multipole fringe, an RF coupler kick and a
-    misaligned collimator whose aperture moves with it -- at the 5 GeV ring
-    energy."""
+    and quadrupoles, the hard-edge multipole fringe, the soft-edge quadrupole
+    fringe, an RF coupler kick and a misaligned collimator whose aperture
+    moves with it -- at the 5 GeV ring energy."""
     E = []
     E.append(L.Element("drift", "D", {"l": 0.5}))
     E.append(L.Element("sbend", "BMIS", {"l": 1.0, "g": 0.02, "e1": 0.03, "e2": 0.01, "x_offset": 1e-4,
@@ -103,6 +103,9 @@ def rare_zoo_lattice() -> L.Lattice:
     E.append(L.Element("quadrupole", "QELEC", {"l": 0.4, "k1": 0.7, "x_offset": 1e-4, "tilt": 0.01},
                        num_steps=4, fringe_type="full", a_pole_elec={1: 3e6}, b_pole_elec={0: 1e5}))
     E.append(L.Element("sextupole", "SHARD", {"l": 0.2, "k2": 30.0}, fringe_type="hard_edge_only"))
+    E.append(L.Element("quadrupole", "QSOFT", {"l": 0.4, "k1": 0.9, "fq1": 2e-3, "fq2": 1e-3}, fringe_type="full"))
+    E.append(L.Element("quadrupole", "QSOFT2", {"l": 0.3, "k1": -1.2, "fq1": 0.05, "fq2": 0.02},
+                       fringe_type="soft_edge_only"))
     E.append(L.Element("rfcavity", "RFCPL", {"l": 0.6, "voltage": 2e6, "phi0": 0.05, "rf_frequency": 499.98e6,
                                              "coupler_strength": 0.05, "coupler_angle": 0.1, "coupler_phase": 0.02},
                        num_steps=6, coupler_at="both_ends"))

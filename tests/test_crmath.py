@@ -1,4 +1,5 @@
-"""The device's correctly rounded transcendentals, compiled for the host.
+"""The device's correctly rounded transcendentals (sin, cos, sinh, cosh, exp,
+asin, atan2), compiled for the host.
 
 bgt_crmath.cuh is host/device code.  Here it is compiled with g++ (no FMA
 contraction, like the device build's --fmad=false) into tests/crmath_check.cpp
