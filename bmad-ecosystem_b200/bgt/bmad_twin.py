@@ -36,7 +36,7 @@ from typing import Dict, List, Optional, Tuple
 from . import lattice as L
 
 _END_NAMES = ("entrance_end", "exit_end", "both_ends", "no_end")
-_FRINGE_NAMES = ("none", "basic_bend", "full", "hard_edge_only", "soft_edge_only")
+_FRINGE_NAMES = ("none", "basic_bend", "full", "hard_edge_only", "soft_edge_only", "sad_full", "linear_edge")
 _APERTURE_NAMES = ("rectangular", "elliptical")
 _SPECIES = {"electron": (L.M_ELECTRON, -1), "positron": (L.M_ELECTRON, 1),
             "proton": (938.27208816e6, 1), "antiproton": (938.27208816e6, -1)}

@@ -44,7 +44,8 @@ KEYS = {
     "vkicker": 34, "rcollimator": 35, "ecollimator": 36, "pipe": 44, "thick_multipole": 67,
 }
 # fringe_type (bmad_struct.f90:164-168)
-FRINGE = {"none": 1, "soft_edge_only": 2, "hard_edge_only": 3, "full": 4, "basic_bend": 7}
+FRINGE = {"none": 1, "soft_edge_only": 2, "hard_edge_only": 3, "full": 4, "sad_full": 5, "linear_edge": 6,
+          "basic_bend": 7}
 # fringe_at / aperture_at (bmad_struct.f90:372)
 ENDS = {"entrance_end": 1, "exit_end": 2, "both_ends": 3, "no_end": 4}
 # aperture_type (bmad_struct.f90:157), 0 = none set

@@ -636,6 +636,34 @@ __device__ __forceinline__ void soft_quad_edge_kick(Part& p, const double* s, bo
   p.py = py * ef1;
 }
 
+// sad_soft_bend_edge_kick, bmad/modules/fringe_mod.f90:892-996 (tracking
+// part, sbend): s = (12 fint hgap, 12 fintx hgapx, g + dg)
+__device__ __forceinline__ void sad_soft_bend_edge(Part& p, const double* s, bool first_edge) {
+  const double fb = first_edge ? s[0] : s[1];
+  if (fb == 0) return;
+  double g = s[2];
+  if (g == 0) return;
+  g = g * 1;
+  if (!first_edge) g = -g;
+  const double px = p.px, y = p.y, rel_p = 1 + p.pz;
+  const double c1 = fb * fb * g / (24 * rel_p);
+  const double c2 = fb * (g * g) / (6 * rel_p);
+  const double c3 = 2 * (g * g) / (3 * fb * rel_p);
+  const double y2 = y * y, y3 = y * y2, y4 = y2 * y2;
+  p.x = p.x + c1 * p.pz;
+  p.py = p.py + c2 * y - c3 * y3;
+  p.z = p.z + (c1 * px + c2 * y2 / 2 - c3 * y4 / 4) / rel_p;
+}
+
+// linear_bend_edge_kick, bmad/modules/fringe_mod.f90:151-212 (tracking
+// part): s = (ht_x, ht_y at the entrance, ht_x, ht_y at the exit)
+__device__ __forceinline__ void linear_bend_edge(Part& p, const double* s, bool first_edge) {
+  const double ht_x = first_edge ? s[0] : s[2], ht_y = first_edge ? s[1] : s[3];
+  const double x = p.x, y = p.y;
+  p.px = p.px + ht_x * x;
+  p.py = p.py + ht_y * y;
+}
+
 // ---------------------------------------------------------------------------
 // Hwang hard-edge bend fringe, bmad/modules/fringe_mod.f90:240-418 (td = +1)
 template <bool ENTERING>

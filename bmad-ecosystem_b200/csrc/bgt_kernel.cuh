@@ -555,9 +555,13 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
     else
       offset_set(p, R.mis, fl, G, m, true);
   }
+  const double* ext = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);  // soft / linear edge constants
   if (fl & F_EDGE_IN) {
-    // apply_element_edge_kick.f90:160-201: entering, magnetic then electric
-    hwang_edge<true>(p, q + B_EDGE);
+    // apply_element_edge_kick.f90:160-201: entering, magnetic (bend_edge_kick,
+    // fringe_mod.f90:39-127) then electric
+    if (RARE && (fl & F_SOFT_EDGE)) sad_soft_bend_edge(p, ext, true);
+    if (!(RARE && (fl & F_NO_HWANG))) hwang_edge<true>(p, q + B_EDGE);
+    if (RARE && (fl & F_LINEAR_EDGE)) linear_bend_edge(p, ext, true);
     if (RARE && (fl & F_ELEC_EDGE)) electric_longitudinal_fringe(p, ae, be, ixe, 1.0, G);
   }
   if (orbit_too_large(p, G)) return;
@@ -634,7 +638,9 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
   if (fl & F_EDGE_OUT) {
     // leaving: electric then magnetic
     if (RARE && (fl & F_ELEC_EDGE)) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
-    hwang_edge<false>(p, q + B_EDGE + EDGE_N);
+    if (RARE && (fl & F_LINEAR_EDGE)) linear_bend_edge(p, ext, false);
+    if (!(RARE && (fl & F_NO_HWANG))) hwang_edge<false>(p, q + B_EDGE + EDGE_N);
+    if (RARE && (fl & F_SOFT_EDGE)) sad_soft_bend_edge(p, ext, false);
   }
   if (fl & F_MISALIGN) {
     if (RARE && (fl & F_BEND_MIS))

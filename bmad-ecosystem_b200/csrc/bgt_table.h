@@ -66,9 +66,16 @@ enum Flag : int32_t {
   // rfcavity coupler kick at the entrance / exit (rf_coupler_kick.f90)
   F_COUPLER_IN = 1 << 22,
   F_COUPLER_OUT = 1 << 23,
-  // quadrupole soft-edge fringe (fringe_type full or soft_edge_only with
-  // fq1 or fq2 nonzero): k1, fq1, fq2 follow the hard-edge strength
+  // soft-edge fringe: a quadrupole's (fringe_type full or soft_edge_only,
+  // fq1 or fq2 nonzero: k1, fq1, fq2 follow the hard-edge strength) or a
+  // bend's SAD soft edge (soft_edge_only, sad_full: fb_in, fb_out, g + dg
+  // after the electric multipoles)
   F_SOFT_EDGE = 1 << 24,
+  // bend linear_edge fringe: ht_x, ht_y at the entrance, then at the exit,
+  // after the electric multipoles
+  F_LINEAR_EDGE = 1 << 25,
+  // bend edges without the Hwang map (soft_edge_only, linear_edge)
+  F_NO_HWANG = 1 << 26,
 };
 
 struct RecHdr {

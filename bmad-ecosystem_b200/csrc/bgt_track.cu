@@ -298,7 +298,7 @@ static void put_edge(double* E, const bgt_element& e, bool entering) {
   double k1 = e.is_on ? e.k1 : 0.0;
   double ang = entering ? e.e1 : e.e2;
   double fint_gap = entering ? e.fint * e.hgap : e.fintx * e.hgapx;
-  if (e.fringe_type == BGT_FRINGE_HARD_EDGE_ONLY) fint_gap = 0;
+  if (e.fringe_type == BGT_FRINGE_HARD_EDGE_ONLY || e.fringe_type == BGT_FRINGE_SAD_FULL) fint_gap = 0;
   double cos_e = cos(ang), sin_e = sin(ang);
   double tan_e = sin_e / cos_e, sec_e = 1 / cos_e;
   double gt = g_tot * tan_e;
@@ -591,9 +591,11 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
         err = ename(e) + ": exact_multipoles is not supported";
         return BGT_EUNSUPPORTED;
       }
-      bool edges = e.fringe_type != BGT_FRINGE_NONE;
-      if (edges && e.fringe_type != BGT_FRINGE_BASIC_BEND && e.fringe_type != BGT_FRINGE_HARD_EDGE_ONLY) {
-        err = ename(e) + ": bend fringe_type other than basic_bend/hard_edge_only is not supported";
+      const int ft = e.fringe_type;
+      bool edges = ft != BGT_FRINGE_NONE;
+      if (edges && ft != BGT_FRINGE_BASIC_BEND && ft != BGT_FRINGE_HARD_EDGE_ONLY && ft != BGT_FRINGE_SAD_FULL &&
+          ft != BGT_FRINGE_SOFT_EDGE_ONLY && ft != BGT_FRINGE_LINEAR_EDGE) {
+        err = ename(e) + ": bend fringe_type full (the exact bend edge) is not supported";
         return BGT_EUNSUPPORTED;
       }
       if (ixe > -1 && !edges && e.fringe_at != BGT_NO_END) {
@@ -662,6 +664,14 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       }
       put_edge(q + B_EDGE, e, true);
       put_edge(q + B_EDGE + EDGE_N, e, false);
+      // bend_edge_kick (fringe_mod.f90:39-127): the Hwang map for basic_bend,
+      // hard_edge_only and sad_full; the SAD soft edge for soft_edge_only and
+      // sad_full (nothing when fint hgap or g + dg is zero); the linear edge
+      if (edges && (ft == BGT_FRINGE_SOFT_EDGE_ONLY || ft == BGT_FRINGE_LINEAR_EDGE)) flags |= F_NO_HWANG;
+      if ((ft == BGT_FRINGE_SOFT_EDGE_ONLY || ft == BGT_FRINGE_SAD_FULL) && e.g + e.dg != 0 &&
+          (12 * e.fint * e.hgap != 0 || 12 * e.fintx * e.hgapx != 0))
+        flags |= F_SOFT_EDGE;
+      if (ft == BGT_FRINGE_LINEAR_EDGE) flags |= F_LINEAR_EDGE;
       if (b1 != 0) flags |= F_K1_BODY;
       else if ((g == 0 && dg == 0) || step_len == 0) flags |= F_DRIFT_BODY;
       if (dg == 0) flags |= F_SEMI_LINEAR_OK;
@@ -694,6 +704,30 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       q[ixe + 1 + n] = e.bn_elec[n];
     }
     if (e.l != 0) flags |= F_ELEC_EDGE;
+  }
+  if (kind == K_BEND && (flags & F_SOFT_EDGE)) {
+    // sad_soft_bend_edge_kick, fringe_mod.f90:913-930
+    double* q = B.ptr_after_push(3);
+    q[0] = 12 * e.fint * e.hgap;
+    q[1] = 12 * e.fintx * e.hgapx;
+    q[2] = e.g + e.dg;
+  }
+  if (kind == K_BEND && (flags & F_LINEAR_EDGE)) {
+    // linear_bend_edge_kick, fringe_mod.f90:170-201 (c_dir = 1)
+    double* q = B.ptr_after_push(4);
+    const double g_tot = e.is_on ? (e.g + e.dg) * 1.0 : 0.0;
+    for (int end = 0; end < 2; end++) {
+      const double ang = end == 0 ? e.e1 : e.e2, fint = end == 0 ? e.fint : e.fintx;
+      const double hgap = end == 0 ? e.hgap : e.hgapx;
+      const double cos_e = cos(ang), sin_e = sin(ang), tan_e = sin_e / cos_e;
+      double ht_x = g_tot * tan_e, ht_y;
+      if (fint == 0)
+        ht_y = -ht_x;
+      else
+        ht_y = -g_tot * tan(ang - 2 * fint * g_tot * hgap * (1 + sin_e * sin_e) / cos_e);
+      q[2 * end] = 1 * ht_x;
+      q[2 * end + 1] = 1 * ht_y;
+    }
   }
   if (kind == K_QUAD || kind == K_THICK_MULT) {
     // init_fringe_info (bmad/low_level/init_fringe_info.f90:22-60); the edge
@@ -869,7 +903,8 @@ static cudaError_t upload_multipole_tables() {
 
 // Whether a compiled record uses a feature only the RARE kernels handle.
 static bool record_is_rare(const RecHdr* rh) {
-  return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS | F_COUPLER_IN | F_COUPLER_OUT)) != 0;
+  return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS | F_COUPLER_IN | F_COUPLER_OUT |
+                       F_SOFT_EDGE | F_LINEAR_EDGE | F_NO_HWANG)) != 0;
 }
 
 // Enqueue tracking of slots on `st`.

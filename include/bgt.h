@@ -45,7 +45,7 @@
  * RF time (bmad_com%absolute_time_tracking = F), magnetic and electric
  * multipoles (electric ones on quadrupoles, sextupoles, octupoles, thick
  * multipoles and bends), misaligned elements including bends, RF coupler
- * kicks, no radiation/spin, no exact bend multipoles, no full / soft bend
+ * kicks, no radiation/spin, no exact bend multipoles, no full (exact) bend
  * fringe.  bgt_create rejects any element outside that scope with
  * BGT_EUNSUPPORTED and names the element.
  */
@@ -84,7 +84,7 @@ enum {
 
 /* fringe_type (bmad_struct.f90:164-168); 1 = none$ */
 enum { BGT_FRINGE_NONE = 1, BGT_FRINGE_SOFT_EDGE_ONLY = 2, BGT_FRINGE_HARD_EDGE_ONLY = 3,
-       BGT_FRINGE_FULL = 4, BGT_FRINGE_BASIC_BEND = 7 };
+       BGT_FRINGE_FULL = 4, BGT_FRINGE_SAD_FULL = 5, BGT_FRINGE_LINEAR_EDGE = 6, BGT_FRINGE_BASIC_BEND = 7 };
 /* fringe_at / aperture_at (bmad_struct.f90:372) */
 enum { BGT_ENTRANCE_END = 1, BGT_EXIT_END = 2, BGT_BOTH_ENDS = 3, BGT_NO_END = 4 };
 /* aperture_type (bmad_struct.f90:157); 0 = no aperture limits set */

@@ -1413,7 +1413,7 @@ void bgo_hwang_bend_edge_kick(const bgo_ele* ele, int entering, bgo_coord* orb, 
     e = ele->e2;
     fint_gap = ele->fintx * ele->hgapx;
   }
-  if (ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY) fint_gap = 0;
+  if (ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY || ele->fringe_type == BGO_FRINGE_SAD_FULL) fint_gap = 0;
   double cos_e = cos(e), sin_e = sin(e);
   double tan_e = sin_e / cos_e, sec_e = 1 / cos_e;
   double gt = g_tot * tan_e;
@@ -1559,6 +1559,60 @@ static void hard_multipole_edge_kick(const bgo_ele* ele, int first_edge, bgo_coo
 
 /* apply_element_edge_kick, bmad/low_level/apply_element_edge_kick.f90:37-278
  * for the bmad_standard field_calc case.  Returns -1 for unsupported forms. */
+/* sad_soft_bend_edge_kick, bmad/modules/fringe_mod.f90:892-996 (tracking
+ * part, sbend): the soft-edge bend fringe of fringe_type soft_edge_only and
+ * sad_full, fb = 12 fint hgap at the entrance (fintx, hgapx at the exit). */
+static void sad_soft_bend_edge_kick(const bgo_ele* ele, int first_edge, bgo_coord* orb) {
+  if (ele->fringe_type != BGO_FRINGE_SOFT_EDGE_ONLY && ele->fringe_type != BGO_FRINGE_SAD_FULL) return;
+  double fb = first_edge ? 12 * ele->fint * ele->hgap : 12 * ele->fintx * ele->hgapx;
+  if (fb == 0) return;
+  double g = ele->g + ele->dg;
+  if (g == 0) return;
+  g = g * 1;
+  if (!first_edge) g = -g;
+  double px = orb->vec[1];
+  double y = orb->vec[2];
+  double rel_p = 1 + orb->vec[5];
+  double c1 = fb * fb * g / (24 * rel_p);
+  double c2 = fb * (g * g) / (6 * rel_p);
+  double c3 = 2 * (g * g) / (3 * fb * rel_p);
+  double y2 = y * y, y3 = y * y2, y4 = y2 * y2;
+  orb->vec[0] = orb->vec[0] + c1 * orb->vec[5];
+  orb->vec[3] = orb->vec[3] + c2 * y - c3 * y3;
+  orb->vec[4] = orb->vec[4] + (c1 * px + c2 * y2 / 2 - c3 * y4 / 4) / rel_p;
+  FL(30);
+}
+
+/* linear_bend_edge_kick, bmad/modules/fringe_mod.f90:151-212 (tracking
+ * part): the linear edge focusing of fringe_type linear_edge. */
+static void linear_bend_edge_kick(const bgo_ele* ele, int first_edge, bgo_coord* orb) {
+  double c_dir = 1.0;
+  double g_tot = ele->is_on ? (ele->g + ele->dg) * c_dir : 0.0;
+  double e, fint, hgap;
+  if (first_edge) {
+    e = ele->e1;
+    fint = ele->fint;
+    hgap = ele->hgap;
+  } else {
+    e = ele->e2;
+    fint = ele->fintx;
+    hgap = ele->hgapx;
+  }
+  double cos_e = cos(e), sin_e = sin(e), tan_e = sin_e / cos_e;
+  double ht_x = g_tot * tan_e, ht_y;
+  if (fint == 0) {
+    ht_y = -ht_x;
+  } else {
+    ht_y = -g_tot * tan(e - 2 * fint * g_tot * hgap * (1 + sin_e * sin_e) / cos_e);
+  }
+  ht_x = 1 * ht_x;
+  ht_y = 1 * ht_y;
+  double x = orb->vec[0], y = orb->vec[2];
+  orb->vec[1] = orb->vec[1] + ht_x * x;
+  orb->vec[3] = orb->vec[3] + ht_y * y;
+  FL(4);
+}
+
 /* soft_quadrupole_edge_kick, bmad/modules/fringe_mod.f90:555-660 (tracking
  * part): the soft-edge fringe of a quadrupole with the fringe integrals
  * fq1, fq2; charge_dir = 1 (forward tracking of the reference species). */
@@ -1613,8 +1667,20 @@ static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first
       if (ele->fringe_type == BGO_FRINGE_NONE) break;
       if (ele->fringe_type == BGO_FRINGE_BASIC_BEND || ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY) {
         bgo_hwang_bend_edge_kick(ele, first_edge, orb, param);
+      } else if (ele->fringe_type == BGO_FRINGE_SAD_FULL) {
+        if (first_edge) {
+          sad_soft_bend_edge_kick(ele, first_edge, orb);
+          bgo_hwang_bend_edge_kick(ele, first_edge, orb, param);
+        } else {
+          bgo_hwang_bend_edge_kick(ele, first_edge, orb, param);
+          sad_soft_bend_edge_kick(ele, first_edge, orb);
+        }
+      } else if (ele->fringe_type == BGO_FRINGE_SOFT_EDGE_ONLY) {
+        sad_soft_bend_edge_kick(ele, first_edge, orb);
+      } else if (ele->fringe_type == BGO_FRINGE_LINEAR_EDGE) {
+        linear_bend_edge_kick(ele, first_edge, orb);
       } else {
-        return -1;
+        return -1; /* full: the exact (PTC) bend edge is not restated */
       }
       break;
     default:

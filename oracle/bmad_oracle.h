@@ -70,7 +70,9 @@ enum {
   BGO_FRINGE_BASIC_BEND = 1,
   BGO_FRINGE_FULL = 2,
   BGO_FRINGE_HARD_EDGE_ONLY = 3,
-  BGO_FRINGE_SOFT_EDGE_ONLY = 4
+  BGO_FRINGE_SOFT_EDGE_ONLY = 4,
+  BGO_FRINGE_SAD_FULL = 5,
+  BGO_FRINGE_LINEAR_EDGE = 6
 };
 
 /* fringe_at / aperture_at values */

@@ -25,7 +25,8 @@ N_POLE = 22
 KEY = {"drift": 1, "quadrupole": 2, "sbend": 3, "sextupole": 4, "octupole": 5, "thick_multipole": 6,
        "multipole": 7, "ab_multipole": 8, "rfcavity": 9, "marker": 10, "ecollimator": 11, "rcollimator": 12,
        "instrument": 13, "monitor": 14, "pipe": 15, "hkicker": 16, "vkicker": 17, "kicker": 18}
-FRINGE = {"none": 0, "basic_bend": 1, "full": 2, "hard_edge_only": 3, "soft_edge_only": 4}
+FRINGE = {"none": 0, "basic_bend": 1, "full": 2, "hard_edge_only": 3, "soft_edge_only": 4, "sad_full": 5,
+          "linear_edge": 6}
 ENDS = {"no_end": 0, "entrance_end": 1, "exit_end": 2, "both_ends": 3}
 APT = {"rectangular": 0, "elliptical": 1, "none": 0}
 

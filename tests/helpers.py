@@ -84,8 +84,9 @@ def rare_zoo_lattice() -> L.Lattice:
     bends (offset_particle's bend geometry, with g, ref_tilt or roll), the
     straight geometry of a misaligned g = 0 bend, electric multipoles in bends
     and quadrupoles, the hard-edge multipole fringe, the soft-edge quadrupole
-    fringe, an RF coupler kick and a misaligned collimator whose aperture
-    moves with it -- at the 5 GeV ring energy."""
+    fringe, the SAD soft and linear bend edges, an RF coupler kick and a
+    misaligned collimator whose aperture moves with it -- at the 5 GeV ring
+    energy."""
     E = []
     E.append(L.Element("drift", "D", {"l": 0.5}))
     E.append(L.Element("sbend", "BMIS", {"l": 1.0, "g": 0.02, "e1": 0.03, "e2": 0.01, "x_offset": 1e-4,
@@ -104,6 +105,12 @@ def rare_zoo_lattice() -> L.Lattice:
                        num_steps=4, fringe_type="full", a_pole_elec={1: 3e6}, b_pole_elec={0: 1e5}))
     E.append(L.Element("sextupole", "SHARD", {"l": 0.2, "k2": 30.0}, fringe_type="hard_edge_only"))
     E.append(L.Element("quadrupole", "QSOFT", {"l": 0.4, "k1": 0.9, "fq1": 2e-3, "fq2": 1e-3}, fringe_type="full"))
+    E.append(L.Element("sbend", "BSOFT", {"l": 1.0, "g": 0.02, "e1": 0.05, "e2": 0.02, "fint": 0.5, "hgap": 0.03},
+                       fringe_type="soft_edge_only"))
+    E.append(L.Element("sbend", "BSAD", {"l": 1.0, "g": -0.015, "e1": 0.08, "fint": 0.4, "hgap": 0.02},
+                       fringe_type="sad_full"))
+    E.append(L.Element("sbend", "BLIN", {"l": 0.8, "g": 0.01, "e1": 0.1, "e2": -0.05, "fint": 0.3, "hgap": 0.02},
+                       fringe_type="linear_edge"))
     E.append(L.Element("quadrupole", "QSOFT2", {"l": 0.3, "k1": -1.2, "fq1": 0.05, "fq2": 0.02},
                        fringe_type="soft_edge_only"))
     E.append(L.Element("rfcavity", "RFCPL", {"l": 0.6, "voltage": 2e6, "phi0": 0.05, "rf_frequency": 499.98e6,
