@@ -12,6 +12,9 @@
   lost_z = 7 and lost_pz = 8: files written by Bmad round-trip through this
   module unchanged.  ``es23.15`` keeps 16 significant digits, so an ASCII
   round trip moves coordinates by up to ~5e-16 relative.
+* The legacy ``!ASCII::3`` format (``write_ascii3_beam`` /
+  ``read_ascii3_beam``), and ``read_beam``, which tells the two apart as
+  ``read_beam_file`` does.
 * Checkpoints (``save_checkpoint`` / ``load_checkpoint``): the exact FP64 /
   int32 arrays and the next turn index in one ``.npz`` file, so that tracking
   resumed from a checkpoint (``turn0`` = the saved turn) is bit-identical to
@@ -265,6 +268,123 @@ def read_ascii_beam(path: str) -> List[BeamBunch]:
                     raise ValueError(f"column name not recognised: {c}")
         out.append(b)
     return out
+
+
+# ---------------------------------------------------------------------------
+# The legacy '!ASCII::3' format: write_beam_file with old_ascii$ and the
+# ASCII::3 branch of read_beam_file (bmad/multiparticle/beam_file_io.f90:76-106,
+# 446-640).  Header: ix_ele, n_bunch, n_particle; per bunch BEGIN_BUNCH, the
+# species, charge_tot, z_center, t_center, one line per particle
+# (6es19.10 coordinates, es14.5 charge, i6 state, 3es19.10 spin, i6 ix_ele,
+# i3 location) and END_BUNCH.  Reading, a particle line needs the six
+# coordinates and may stop after any later field; lines beyond n_particle
+# are skipped.  p0c is not part of the format: the caller gives it.
+
+def write_ascii3_beam(path: str, bunches: List[BeamBunch], new_file: bool = True) -> None:
+    with open(path, "w" if new_file else "a") as f:
+        if new_file:
+            f.write("!ASCII::3\n")
+        first = bunches[0] if bunches else None
+        ix_ele = int(first.ix_ele[0]) if first is not None and first.n else 0
+        f.write(f"  {ix_ele}  ! ix_ele\n  {len(bunches)}  ! n_bunch\n  {first.n if first else 0}  ! n_particle\n")
+        for b in bunches:
+            loc = LOCATION_NAME.index(b.location) if b.location in LOCATION_NAME else 2
+            charge_tot = b.charge_tot if b.charge_tot is not None else float(np.sum(b.charge))
+            f.write(" BEGIN_BUNCH\n")
+            f.write(f"   {b.species}\n")
+            f.write(f"  {charge_tot!r}  ! charge_tot\n  0.0  ! z_center\n  0.0  ! t_center\n")
+            for j in range(b.n):
+                f.write("".join(f"{v:19.10E}" for v in b.vec6[:, j]) + f"{b.charge[j]:14.5E}{int(b.state[j]):6d}" +
+                        "".join(f"{v:19.10E}" for v in b.spin[:, j]) + f"{int(b.ix_ele[j]):6d}{loc:3d}\n")
+            f.write(" END_BUNCH\n")
+
+
+def read_ascii3_beam(path: str, p0c: float = 0.0) -> List[BeamBunch]:
+    words = []
+    for ln in open(path).read().splitlines():
+        if ln.strip().upper().startswith("!ASCII::3"):
+            continue
+        body = ln.split("!", 1)[0].strip()
+        if body:
+            words.append(body)
+    it = iter(words)
+
+    def nxt(what):
+        try:
+            return next(it)
+        except StopIteration:
+            raise ValueError(f"beam file ends before the {what}") from None
+
+    ix_ele = int(_float(nxt("ix_ele")))
+    n_bunch = int(_float(nxt("n_bunch")))
+    n_particle = int(_float(nxt("n_particle")))
+    out = []
+    for _ in range(n_bunch):
+        if "BEGIN_BUNCH" not in nxt("BEGIN_BUNCH marker").upper():
+            raise ValueError('no "BEGIN_BUNCH" marker found')
+        species = nxt("species").split()[0]
+        try:
+            _float(species)
+            numeric = True
+        except ValueError:
+            numeric = False
+        if numeric:
+            raise ValueError("old style format does not include the bunch species")
+        charge_tot = _float(nxt("charge_tot"))
+        nxt("z_center")
+        nxt("t_center")
+        vec = np.zeros((6, n_particle))
+        charge = np.zeros(n_particle)
+        state = np.ones(n_particle, np.int32)
+        spin = np.zeros((3, n_particle))
+        ixe = np.full(n_particle, ix_ele, np.int32)
+        loc = 2
+        j = 0
+        while True:
+            ln = nxt("END_BUNCH marker")
+            if "END_BUNCH" in ln.upper():
+                break
+            if j >= n_particle:
+                j += 1
+                continue
+            tok = ln.replace("(", " ").replace(")", " ").replace(",", " ").split()
+            if len(tok) < 6:
+                raise ValueError(f"particle line with fewer than 6 coordinates: {ln!r}")
+            vec[:, j] = [_float(t) for t in tok[:6]]
+            if len(tok) > 6:
+                charge[j] = _float(tok[6])
+            if len(tok) > 7:
+                state[j] = int(tok[7])
+            if len(tok) > 10:
+                spin[:, j] = [_float(t) for t in tok[8:11]]
+            if len(tok) > 11:
+                ixe[j] = int(tok[11])
+            if len(tok) > 12:
+                loc = int(tok[12])
+            j += 1
+        if j < n_particle:
+            raise ValueError(f"bunch has {j} particle lines for n_particle = {n_particle}")
+        out.append(BeamBunch(vec, state, np.full(n_particle, p0c), np.zeros(n_particle), np.zeros(n_particle),
+                             charge, spin, ixe, None, species.lower(), LOCATION_NAME[loc], charge_tot=charge_tot))
+    return out
+
+
+def read_beam(path: str, p0c: float = 0.0) -> List[BeamBunch]:
+    """A beam file in either ASCII format, told apart as read_beam_file does
+    (beam_file_io.f90:455-476): '!ASCII::3' (or a first line that is not a
+    '#' header) is the legacy format, '#' starts the current one; binary
+    files are refused.  p0c is used by the legacy format only."""
+    with open(path) as f:
+        first = ""
+        for ln in f:
+            if ln.strip():
+                first = ln
+                break
+    if "!BINARY" in first or "!BIN::" in first:
+        raise ValueError("binary beam files are not supported")
+    if first.startswith("#"):
+        return read_ascii_beam(path)
+    return read_ascii3_beam(path, p0c)
 
 
 def save_checkpoint(path: str, bunch: Bunch, next_turn: int, **meta):

@@ -89,3 +89,58 @@ def test_checkpoint_is_exact(tmp_path):
     assert turn == 1234 and str(meta["lattice"]) == "fodo64"
     for k in ("vec6", "beta", "state", "ix_ele_lost", "ix_turn_lost"):
         assert np.array_equal(getattr(c, k), getattr(b, k)) and getattr(c, k).dtype == getattr(b, k).dtype
+
+
+def test_legacy_ascii3_round_trip(tmp_path):
+    rng = np.random.default_rng(5)
+    n = 40
+    vec = rng.standard_normal((6, n)) * 1e-3
+    state = np.ones(n, np.int32)
+    state[::7] = B.STATE_NAME.index("Lost_Pos_Y")
+    b = B.BeamBunch(vec, state, np.full(n, 5e9), np.zeros(n), np.zeros(n), np.full(n, 1e-15),
+                          rng.standard_normal((3, n)), np.arange(n, dtype=np.int32), None, "electron",
+                          charge_tot=4e-14)
+    f = tmp_path / "beam3.dat"
+    B.write_ascii3_beam(str(f), [b, b])
+    assert f.read_text().startswith("!ASCII::3")
+    back = B.read_beam(str(f), p0c=5e9)
+    assert len(back) == 2
+    for r in back:
+        assert r.species == "electron" and r.charge_tot == 4e-14
+        assert np.allclose(r.vec6, vec, rtol=1e-10, atol=0)
+        assert np.array_equal(r.state, state) and np.array_equal(r.ix_ele, b.ix_ele)
+        assert np.allclose(r.spin, b.spin, rtol=1e-10) and np.all(r.p0c == 5e9)
+
+
+def test_legacy_ascii3_short_lines_and_extra_particles(tmp_path):
+    f = tmp_path / "short.dat"
+    f.write_text("""!ASCII::3
+ 5   ! ix_ele
+ 1   ! n_bunch
+ 2   ! n_particle
+ BEGIN_BUNCH
+   positron
+ 1e-12  ! charge_tot
+ 0.0  ! z_center
+ 0.0  ! t_center
+ 1e-3 2e-4 -1e-3 0 0.01 1e-3
+ 2e-3 0 0 0 0 0  1.0E-15  6
+ 9 9 9 9 9 9
+ END_BUNCH
+""")
+    (b,) = B.read_beam(str(f), p0c=1e9)
+    assert b.n == 2 and b.species == "positron"
+    assert np.array_equal(b.vec6[:, 0], [1e-3, 2e-4, -1e-3, 0, 0.01, 1e-3])
+    assert b.state[0] == 1 and b.state[1] == 6 and b.charge[1] == 1e-15
+    assert np.all(b.ix_ele == 5)
+
+
+def test_read_beam_tells_the_formats_apart(tmp_path):
+    bunch = Bunch.from_vec(np.full((6, 3), 1e-3), 1e9, B.SPECIES_MASS["electron"])
+    f = tmp_path / "new.dat"
+    B.write_ascii_beam(str(f), [B.BeamBunch.from_bunch(bunch, 1e9)])
+    assert B.read_beam(str(f))[0].n == 3
+    g = tmp_path / "bin.dat"
+    g.write_text("!BIN::3\n")
+    with pytest.raises(ValueError, match="binary"):
+        B.read_beam(str(g))
