@@ -34,6 +34,38 @@ def _key(tracker, n: int, lossy: bool) -> str:
     return f"{tracker.lattice.name}:{tracker.table_bytes()}:{tracker.n_variants}:{n}:{int(lossy)}"
 
 
+def candidates(shapes: Iterable[Tuple[int, int]] = SHAPES, compact_options: Iterable[int] = (0,)) -> list:
+    """The tunings tried: every compiled shape with each compaction
+    interval, and, for the shapes also compiled for global-memory tables,
+    the table in shared memory (0) or in global memory with CTA tiles (2)
+    or warp tiles (3); shapes compiled only for global-memory tables last."""
+    shapes = list(shapes)
+    compact_options = list(compact_options)
+    out = [dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0, table_mode=tm)
+           for (tpb, bps) in shapes for ce in compact_options
+           for tm in ((0, 2, 3) if (tpb, bps) in GLOBAL_TABLE_SHAPES else (0,))]
+    out += [dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=0, turns_per_launch=0, table_mode=tm)
+            for (tpb, bps) in GLOBAL_TABLE_SHAPES if (tpb, bps) not in shapes for tm in (2, 3)]
+    return out
+
+
+def _cuda_timer(tracker, vec6: np.ndarray, pick: np.ndarray, variant: Optional[np.ndarray], turns: int):
+    """A function timing the tracker's current tuning on the sample
+    vec6[:, pick] (CUDA events on the launching stream, best of two)."""
+    import torch
+
+    m = len(pick)
+    dev = torch.device("cuda", tracker.device)
+    base = torch.tensor(np.ascontiguousarray(vec6[:, pick]), dtype=torch.float64, device=dev)
+    var_t = (torch.tensor(np.ascontiguousarray(variant[pick], dtype=np.int32), device=dev)
+             if variant is not None else None)
+    pz = base[5]
+    pc = (1 + pz) * tracker.p0c
+    beta0 = pc / torch.sqrt(pc * pc + tracker.species.mass ** 2)
+    stream = torch.cuda.current_stream(dev)
+    return lambda: _time_shape(tracker, base, beta0, var_t, m, turns, stream, dev)
+
+
 def _time_shape(tracker, base, beta0, var_t, m, turns, stream, dev) -> float:
     import torch
 
@@ -56,13 +88,13 @@ def _time_shape(tracker, base, beta0, var_t, m, turns, stream, dev) -> float:
 
 def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, int]] = SHAPES,
          compact_options: Iterable[int] = (0,), sample: int = 200_000, cache_file: Optional[str] = None,
-         verbose: bool = False, variant: Optional[np.ndarray] = None) -> dict:
+         verbose: bool = False, variant: Optional[np.ndarray] = None, timer=None) -> dict:
     """Pick the fastest tuning for tracking `vec6` (6, n) with `tracker`;
     sets it on the tracker and returns it.  `variant` (sorted int32 [n])
     assigns the particles to lattice variants; the sample is then spread
-    evenly over the bunch so that every variant's share is represented."""
-    import torch
-
+    evenly over the bunch so that every variant's share is represented.
+    `timer` (no arguments, milliseconds of the tracker's current tuning)
+    replaces the CUDA timing of the sample."""
     n = vec6.shape[1]
     lossy = any(c > 0 for c in compact_options)
     key = _key(tracker, n, lossy)
@@ -76,26 +108,14 @@ def tune(tracker, vec6: np.ndarray, turns: int = 4, shapes: Iterable[Tuple[int, 
         return _cache[key]["tuning"]
 
     m = min(n, sample)
-    dev = torch.device("cuda", tracker.device)
     pick = np.linspace(0, n - 1, m).astype(np.int64) if variant is not None else np.arange(m)
-    base = torch.tensor(np.ascontiguousarray(vec6[:, pick]), dtype=torch.float64, device=dev)
-    var_t = (torch.tensor(np.ascontiguousarray(variant[pick], dtype=np.int32), device=dev)
-             if variant is not None else None)
-    pz = base[5]
-    pc = (1 + pz) * tracker.p0c
-    beta0 = pc / torch.sqrt(pc * pc + tracker.species.mass ** 2)
-    stream = torch.cuda.current_stream(dev)
+    if timer is None:
+        timer = _cuda_timer(tracker, vec6, pick, variant, turns)
     results = []
-    shapes = list(shapes)
-    cands = [(tpb, bps, ce, tm) for (tpb, bps) in shapes for ce in compact_options
-             for tm in ((0, 2, 3) if (tpb, bps) in GLOBAL_TABLE_SHAPES else (0,))]
-    # shapes compiled only for global-memory tables
-    cands += [(tpb, bps, 0, tm) for (tpb, bps) in GLOBAL_TABLE_SHAPES if (tpb, bps) not in shapes for tm in (2, 3)]
-    for (tpb, bps, ce, tm) in cands:
-        tun = dict(threads_per_block=tpb, blocks_per_sm=bps, compact_every=ce, turns_per_launch=0, table_mode=tm)
+    for tun in candidates(shapes, compact_options):
         tracker.set_tuning(**tun)
         try:
-            best = _time_shape(tracker, base, beta0, var_t, m, turns, stream, dev)
+            best = timer()
         except _lib.BgtError:
             continue  # shape not available for this table (e.g. table larger than shared memory)
         results.append((best, tun))
