@@ -12,9 +12,16 @@
 // CTA compacts its surviving particles onto the lowest lanes (warp ballot +
 // block prefix sum through shared memory) so dead lanes stop costing issue
 // slots; fully dead warps skip the element loop.
+//
+// Everything up to track1_rec is per-particle arithmetic with no CUDA
+// construct beyond the __device__ qualifiers; a plain C++ compiler that
+// defines those away compiles it for the host (the tests run the element
+// maps that way).  The kernel and its launcher need nvcc.
 #pragma once
 
+#ifdef __CUDACC__
 #include <cuda_runtime.h>
+#endif
 #include <math.h>
 #include <stdint.h>
 
@@ -696,6 +703,7 @@ __device__ __forceinline__ void track1_rec(Part& p, const double* rec, const Glo
   }
 }
 
+#ifdef __CUDACC__
 // ===========================================================================
 // TMA bulk copy + mbarrier (inline PTX, sm_90+ forms valid on sm_100a).
 
@@ -1074,5 +1082,6 @@ struct TrackKernelGroup {
 };
 constexpr int N_KERNEL_GROUPS = 10;
 TrackKernelGroup track_kernel_group(int g);
+#endif  // __CUDACC__
 
 }  // namespace bgt

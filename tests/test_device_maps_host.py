@@ -1,0 +1,214 @@
+"""The tracking kernel's element maps, compiled for the host, against the
+oracle -- without a GPU.
+
+tests/device_maps_host.cpp builds the per-particle part of bgt_kernel.cuh
+(decode, the element bodies, track1_rec and everything they call) with g++
+and -ffp-contract=off, the host counterpart of the device build's
+--fmad=false, on tables from the same compiler bgt_create runs
+(bgt_compile.h).  IEEE division and square root are correctly rounded on
+both sides and every transcendental of a particle coordinate goes through
+the correctly rounded bgt::cr, so the host build performs the device's
+arithmetic bit for bit: these tests hold the device source to the "cr"
+oracle on every machine, the GPU parity suite (test_gpu_parity.py) then
+shows that the GPU runs it the same way.  A second build with
+AddressSanitizer checks that no map reads outside its table.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from bgt import _lib
+from bgt import lattice as L
+from bgt import rings
+from bgt.track import Bunch
+
+from helpers import oracle_track_elements, random_particles, rare_zoo_lattice, zoo_lattice
+
+ROOT = Path(__file__).resolve().parents[1]
+SRC = ROOT / "tests" / "device_maps_host.cpp"
+CXXFLAGS = ["-O2", "-ffp-contract=off", "-std=c++17", "-fPIC", "-shared", "-Wno-unknown-pragmas"]
+
+
+def _build(out: Path, extra=()) -> Path:
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    subprocess.run([gxx, *CXXFLAGS, *extra, "-o", str(out), str(SRC)], check=True, capture_output=True)
+    return out
+
+
+class HostMaps:
+    """bgt_create's tables and the kernel's element maps, run on the host."""
+
+    def __init__(self, lattices, so: Path):
+        self.lats = [lattices] if isinstance(lattices, L.Lattice) else list(lattices)
+        self.lib = C.CDLL(str(so))
+        f = self.lib.dmh_track
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                      C.c_int32, C.c_char_p, C.c_int32]
+        self.lib.dmh_needs_rare.restype = C.c_int
+        self.lib.dmh_needs_rare.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
+        self.n_ele = len(self.lats[0].elements)
+        self.arr = (_lib.BgtElement * (self.n_ele * len(self.lats)))()
+        for v, lat in enumerate(self.lats):
+            for i, e in enumerate(lat.elements):
+                self.arr[v * self.n_ele + i] = _lib.to_bgt_element(e)
+        lat0 = self.lats[0]
+        self.sp = _lib.BgtSpecies(lat0.species.mass, lat0.species.charge, 1, 1e3)
+
+    @property
+    def needs_rare(self) -> bool:
+        rc = self.lib.dmh_needs_rare(C.addressof(self.arr), self.n_ele, len(self.lats), C.addressof(self.sp))
+        assert rc >= 0
+        return rc == 1
+
+    def make_bunch(self, v0) -> Bunch:
+        return Bunch.from_vec(v0, self.lats[0].p0c, self.lats[0].species.mass)
+
+    def track(self, b: Bunch, rec_begin=0, rec_end=None, turn0=0, n_turns=1, variant=None, kernel=0,
+              turns=True):
+        rec_end = self.n_ele if rec_end is None else rec_end
+        var = None if variant is None else np.ascontiguousarray(variant, np.int32)
+        err = C.create_string_buffer(512)
+        rc = self.lib.dmh_track(C.addressof(self.arr), self.n_ele, len(self.lats), C.addressof(self.sp),
+                                None if var is None else var.ctypes.data, b.vec6.ctypes.data, b.beta.ctypes.data,
+                                b.state.ctypes.data, b.ix_ele_lost.ctypes.data,
+                                b.ix_turn_lost.ctypes.data if turns else None, b.n, rec_begin, rec_end, turn0,
+                                n_turns, kernel, err, 512)
+        assert rc == 0, (rc, err.value)
+        return b
+
+
+@pytest.fixture(scope="module")
+def so(tmp_path_factory):
+    return _build(tmp_path_factory.mktemp("dmh") / "libdmh.so")
+
+
+def assert_bitwise(b, ov, ob, ost, oie, oit=None, what=""):
+    assert np.array_equal(b.state, ost), f"{what}: state"
+    assert np.array_equal(b.ix_ele_lost, oie), f"{what}: loss element"
+    if oit is not None:
+        assert np.array_equal(b.ix_turn_lost, oit), f"{what}: loss turn"
+    assert np.array_equal(b.vec6, ov), f"{what}: coordinates differ (max abs {np.max(np.abs(b.vec6 - ov))})"
+    assert np.array_equal(b.beta, ob), f"{what}: beta"
+
+
+@pytest.mark.parametrize("make", [zoo_lattice, rare_zoo_lattice], ids=["zoo", "rare_zoo"])
+@pytest.mark.parametrize("kernel", [0, 1], ids=["picked", "rare"])
+def test_each_element_track1_bitwise(so, oracle_lib, make, kernel):
+    """track1 through every element of both zoos (all element kinds,
+    misalignments, bend geometry, electric fields, edge fringe, couplers,
+    apertures), in the kernel instance the host picks and in the RARE one."""
+    lat = make()
+    hm = HostMaps(lat, so)
+    assert hm.needs_rare == (make is rare_zoo_lattice)
+    v0 = random_particles(512, seed=31)
+    for pos, ele in enumerate(lat.elements):
+        b = hm.track(hm.make_bunch(v0.copy()), pos, pos + 1, kernel=kernel, turns=False)
+        ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
+        assert_bitwise(b, ov, ob, ost, oie, what=ele.name)
+
+
+@pytest.mark.parametrize("make", [zoo_lattice, rare_zoo_lattice], ids=["zoo", "rare_zoo"])
+def test_turns_with_losses(so, oracle_lib, make):
+    lat = make()
+    hm = HostMaps(lat, so)
+    # neither line closes: the orbit grows turn by turn and particles are
+    # lost in every one of the four turns
+    v0 = random_particles(1024, seed=32, scale=0.25)
+    b = hm.track(hm.make_bunch(v0.copy()), n_turns=4)
+    ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), 4, variant="cr")
+    assert len(np.unique(oit[ost != L.ALIVE])) == 4
+    assert_bitwise(b, ov, ob, ost, oie, oit, what=f"{lat.name}, 4 turns")
+
+
+def test_ring_turns_with_apertures_and_start_turn(so, oracle_lib):
+    """The 769-element FODO ring with apertures: 40 turns from turn 7,
+    losses at quads and the RF; loss turns are absolute."""
+    lat = rings.fodo_ring(apertures=True)
+    hm = HostMaps(lat, so)
+    assert not hm.needs_rare
+    v0 = rings.gaussian_beam(rings.BeamSpec(200, 4e-6, 2e-6, 3e-3, 2e-3, seed=77))
+    b = hm.track(hm.make_bunch(v0.copy()), turn0=7, n_turns=40)
+    ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), 40, variant="cr")
+    oit = np.where(ost != L.ALIVE, oit + 7, oit)
+    assert (ost != L.ALIVE).sum() > 20
+    assert_bitwise(b, ov, ob, ost, oie, oit, "ring, 40 turns")
+
+
+def test_error_variants_batched(so, oracle_lib):
+    """Error variants of the ring (misaligned quads and sextupoles with
+    multipole errors), particles interleaved over four variants."""
+    lats = rings.error_variants(4, seed=5)
+    hm = HostMaps(lats, so)
+    n = 240
+    v0 = random_particles(n, seed=33, scale=0.5)
+    var = np.arange(n, dtype=np.int32) % 4
+    b = hm.track(hm.make_bunch(v0.copy()), n_turns=3, variant=var)
+    for v in range(4):
+        m = var == v
+        ov, ob, ost, oie, oit = oracle_track_elements(lats[v], v0[:, m], 0, len(lats[v]), 3, variant="cr")
+        sub = Bunch(b.vec6[:, m], b.beta[m], b.state[m], b.ix_ele_lost[m], b.ix_turn_lost[m])
+        assert_bitwise(sub, ov, ob, ost, oie, oit, f"variant {v}")
+
+
+def test_lost_input_particles_are_left_alone(so):
+    lat = rings.fodo_ring(apertures=True)
+    hm = HostMaps(lat, so)
+    v0 = random_particles(30, seed=34)
+    b = hm.make_bunch(v0.copy())
+    b.state[::3] = L.LOST_NEG_X
+    b.ix_ele_lost[::3] = 7
+    b.ix_turn_lost[::3] = 2
+    hm.track(b, turn0=3, n_turns=2)
+    assert np.array_equal(b.vec6[:, ::3], v0[:, ::3])
+    assert np.all(b.state[::3] == L.LOST_NEG_X) and np.all(b.ix_ele_lost[::3] == 7)
+    assert np.all(b.ix_turn_lost[::3] == 2)
+
+
+_ASAN_CHILD = r"""
+import sys
+sys.path[:0] = [{root!r} + "/bmad-ecosystem_b200", {root!r} + "/tests", {root!r}]
+import numpy as np
+from test_device_maps_host import HostMaps
+from helpers import random_particles, rare_zoo_lattice, zoo_lattice
+from bgt import rings
+from pathlib import Path
+so = Path({so!r})
+for lat in (zoo_lattice(), rare_zoo_lattice()):
+    hm = HostMaps(lat, so)
+    for kernel in (0, 1):
+        v0 = random_particles(64, seed=35, scale=3.0)
+        hm.track(hm.make_bunch(v0), n_turns=2, kernel=kernel)
+hm = HostMaps(rings.error_variants(2, seed=6), so)
+v0 = random_particles(16, seed=36)
+hm.track(hm.make_bunch(v0), n_turns=1, variant=np.arange(16, dtype=np.int32) % 2)
+print("ASAN-CLEAN")
+"""
+
+
+def test_no_read_outside_the_tables_under_asan(tmp_path):
+    """Every element kind of both zoos, each table in a buffer of its own
+    size, under AddressSanitizer: a map that read past its record's table
+    would abort the child process."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    asan = subprocess.run([gxx, "-print-file-name=libasan.so"], capture_output=True, text=True).stdout.strip()
+    if not asan or not os.path.isabs(asan) or not os.path.exists(asan):
+        pytest.skip("libasan not available")
+    so = _build(tmp_path / "libdmh_asan.so", ["-fsanitize=address", "-fno-omit-frame-pointer", "-g", "-O1"])
+    env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=0:exitcode=99")
+    r = subprocess.run([sys.executable, "-c", _ASAN_CHILD.format(root=str(ROOT), so=str(so))], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "ASAN-CLEAN" in r.stdout, (r.returncode, r.stderr[-3000:])
