@@ -594,8 +594,8 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       const int ft = e.fringe_type;
       bool edges = ft != BGT_FRINGE_NONE;
       if (edges && ft != BGT_FRINGE_BASIC_BEND && ft != BGT_FRINGE_HARD_EDGE_ONLY && ft != BGT_FRINGE_SAD_FULL &&
-          ft != BGT_FRINGE_SOFT_EDGE_ONLY && ft != BGT_FRINGE_LINEAR_EDGE) {
-        err = ename(e) + ": bend fringe_type full (the exact bend edge) is not supported";
+          ft != BGT_FRINGE_SOFT_EDGE_ONLY && ft != BGT_FRINGE_LINEAR_EDGE && ft != BGT_FRINGE_FULL) {
+        err = ename(e) + ": bend fringe_type " + std::to_string(ft) + " is not supported";
         return BGT_EUNSUPPORTED;
       }
       if (ixe > -1 && !edges && e.fringe_at != BGT_NO_END) {
@@ -666,8 +666,11 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       put_edge(q + B_EDGE + EDGE_N, e, false);
       // bend_edge_kick (fringe_mod.f90:39-127): the Hwang map for basic_bend,
       // hard_edge_only and sad_full; the SAD soft edge for soft_edge_only and
-      // sad_full (nothing when fint hgap or g + dg is zero); the linear edge
-      if (edges && (ft == BGT_FRINGE_SOFT_EDGE_ONLY || ft == BGT_FRINGE_LINEAR_EDGE)) flags |= F_NO_HWANG;
+      // sad_full (nothing when fint hgap or g + dg is zero); the linear edge;
+      // for full the exact edge inside the k1 hard-edge multipole fringe
+      if (edges && (ft == BGT_FRINGE_SOFT_EDGE_ONLY || ft == BGT_FRINGE_LINEAR_EDGE || ft == BGT_FRINGE_FULL))
+        flags |= F_NO_HWANG;
+      if (ft == BGT_FRINGE_FULL && (flags & (F_EDGE_IN | F_EDGE_OUT))) flags |= F_EXACT_EDGE;
       if ((ft == BGT_FRINGE_SOFT_EDGE_ONLY || ft == BGT_FRINGE_SAD_FULL) && e.g + e.dg != 0 &&
           (12 * e.fint * e.hgap != 0 || 12 * e.fintx * e.hgapx != 0))
         flags |= F_SOFT_EDGE;
@@ -711,6 +714,34 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     q[0] = 12 * e.fint * e.hgap;
     q[1] = 12 * e.fintx * e.hgapx;
     q[2] = e.g + e.dg;
+  }
+  if (kind == K_BEND && (flags & F_EXACT_EDGE)) {
+    // exact_bend_edge_kick, fringe_mod.f90:1486-1511 (time_dir = 1) and the
+    // strength of hard_multipole_edge_kick (fringe_mod.f90:737-738, 772-774)
+    double* q = B.ptr_after_push(XE_N);
+    const double beta0 = e.p0c / e.e_tot;
+    q[XE_BETA0] = beta0;
+    q[XE_IB] = 1 / beta0;
+    q[XE_IB2] = 1 / (beta0 * beta0);
+    const double g_tot = e.is_on ? e.g + e.dg : 0.0;
+    q[XE_GTOT] = g_tot;
+    q[XE_K1] = e.k1;
+    for (int end = 0; end < 2; end++) {
+      double* E = q + (end == 0 ? XE_IN : XE_OUT);
+      const double a = 1 * (end == 0 ? e.e1 : e.e2);
+      E[XE_A] = a;
+      E[XE_TANA] = tan(a);
+      E[XE_COSA] = cos(a);
+      E[XE_SINA] = sin(a);
+      E[XE_NA] = -a;
+      E[XE_TANNA] = tan(-a);
+      E[XE_COSNA] = cos(-a);
+      E[XE_SINNA] = sin(-a);
+      E[XE_SIN2NA] = sin(2.0 * -a);
+      E[XE_B] = end == 0 ? g_tot : -g_tot;
+      E[XE_FINT] = 1 * (end == 0 ? e.fint : e.fintx);
+      E[XE_HGAP] = end == 0 ? e.hgap : e.hgapx;
+    }
   }
   if (kind == K_BEND && (flags & F_LINEAR_EDGE)) {
     // linear_bend_edge_kick, fringe_mod.f90:170-201 (c_dir = 1)
@@ -804,7 +835,7 @@ static void c_multi_tables(double cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1],
 // Whether a compiled record uses a feature only the RARE kernels handle.
 static bool record_is_rare(const RecHdr* rh) {
   return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS | F_COUPLER_IN | F_COUPLER_OUT |
-                       F_SOFT_EDGE | F_LINEAR_EDGE | F_NO_HWANG)) != 0;
+                       F_SOFT_EDGE | F_LINEAR_EDGE | F_NO_HWANG | F_EXACT_EDGE)) != 0;
 }
 
 // The element tables of all variants, as bgt_create uploads them.  Per

@@ -278,6 +278,21 @@ BGT_HD void sincos(double x, double* s, double* c) {
   *c = cr::cos(x);
 }
 
+// ---- tan (|x| < 2^19; larger or non-finite arguments use the library) ----
+// Below 2^-27, x^3/3 is below half an ulp of x, so the correctly rounded
+// value is x.  Elsewhere sin / cos of the double-double reduced argument,
+// divided in double-double: the relative error stays far below the 2^-53
+// rounding step except within a few 1e-20 of the poles, which no tracking
+// argument reaches.  Used by the exact (PTC) bend edge only.
+BGT_HD_NOINLINE double tan(double x) {
+  if (!(fabs(x) < 524288.0)) return ::tan(x);
+  if (fabs(x) < 0x1p-27) return x;
+  dd s, c;
+  dd_sincos_any(x, &s, &c);
+  dd t = dd_div(s, c);
+  return t.hi + t.lo;
+}
+
 // ---- sinh / cosh (|x| <= 2; larger arguments use the library) ----
 
 BGT_HD_NOINLINE dd dd_sinh_kernel(double x) {
@@ -515,6 +530,10 @@ BGT_HD double atan2(double y, double x) {
   if (x < 0) a = (y >= 0) ? dd_add(a, dd{BGT_CR_PI_HI, BGT_CR_PI_LO}) : dd_add(a, dd_neg(dd{BGT_CR_PI_HI, BGT_CR_PI_LO}));
   return a.hi + a.lo;
 }
+
+// atan(x) = atan2(x, 1): the quotient x / 1 is exact, so the correctly
+// rounded atan2 is the correctly rounded atan.
+BGT_HD double atan(double x) { return cr::atan2(x, 1.0); }
 
 }  // namespace cr
 }  // namespace bgt

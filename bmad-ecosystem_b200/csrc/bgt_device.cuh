@@ -46,6 +46,13 @@ struct DriftMemo {
   double a;
 };
 
+// Out-of-line device functions (a plain static function in a host build).
+#ifdef __CUDACC__
+#define BGT_DEV_NOINLINE __device__ __noinline__
+#else
+#define BGT_DEV_NOINLINE static __attribute__((noinline))
+#endif
+
 __device__ __forceinline__ double sq(double x) { return x * x; }
 
 // sim_utils/special_functions/sqrt_one.f90:18-40
@@ -662,6 +669,137 @@ __device__ __forceinline__ void linear_bend_edge(Part& p, const double* s, bool 
   const double x = p.x, y = p.y;
   p.px = p.px + ht_x * x;
   p.py = p.py + ht_y * y;
+}
+
+// ---------------------------------------------------------------------------
+// The exact (PTC) bend edge of fringe_type full, exact_bend_edge_kick,
+// bmad/modules/fringe_mod.f90:1465-1686 (tracking part, time_dir = 1).  The
+// particle goes to PTC's (x, px, y, py, pt, ct), through a rotation of the
+// frame by the edge angle, the dipole fringe map and the wedge of the bend
+// field, and back.  xe is the exact-edge block (XE_*), E one end's part of
+// it.  The steps return false where the reference sets err_flag.
+
+// ptc_rot_xz, fringe_mod.f90:1384-1441 (a, tan a, cos a, sin a)
+__device__ __forceinline__ bool ptc_rot_xz(double* X, double tan_a, double cos_a, double sin_a, const double* xe) {
+  const double beta0 = xe[XE_BETA0];
+  double arg = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[1] * X[1] - X[3] * X[3];
+  if (arg < 0) return false;
+  double pz = sqrt(arg);
+  double pt = 1.0 - X[1] * tan_a / pz;
+  double x1 = X[0];
+  X[0] = x1 / cos_a / pt;
+  X[1] = X[1] * cos_a + sin_a * pz;
+  X[2] = X[2] + X[3] * x1 * tan_a / pz / pt;
+  X[5] = X[5] + x1 * tan_a / pz / pt * (xe[XE_IB] + X[4]);
+  return true;
+}
+
+// ptc_wedger, fringe_mod.f90:1020-1123, for the end's angle -a and b1 =
+// g_tot != 0 (g_tot = 0 is a rotation by -a)
+__device__ __forceinline__ bool ptc_wedge(double* X, const double* E, const double* xe) {
+  const double beta0 = xe[XE_BETA0], b1 = xe[XE_GTOT];
+  const double a = E[XE_NA], cos_a = E[XE_COSNA], sin_a = E[XE_SINNA];
+  double fac = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[1] * X[1] - X[3] * X[3];
+  if (fac < 0) return false;
+  double radix = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[3] * X[3];
+  if (radix < 1e-10) return false;
+  double pz = sqrt(fac), pt = sqrt(radix);
+  double Xn2 = X[1] * cos_a + (pz - b1 * X[0]) * sin_a;
+  radix = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - Xn2 * Xn2 - X[3] * X[3];
+  if (radix < 1e-10) return false;
+  double pzs = sqrt(radix);
+  double Xn1 = X[0] * cos_a + (X[0] * X[1] * E[XE_SIN2NA] + (sin_a * sin_a) * (2.0 * X[0] * pz - b1 * (X[0] * X[0]))) /
+                                  (pzs + pz * cos_a - X[1] * sin_a);
+  double Xn3 = (a + cr::asin(X[1] / pt) - cr::asin(Xn2 / pt)) / b1;
+  double Xn6 = X[5] + Xn3 * (xe[XE_IB] + X[4]);
+  Xn3 = X[2] + X[3] * Xn3;
+  X[0] = Xn1;
+  X[1] = Xn2;
+  X[2] = Xn3;
+  X[5] = Xn6;
+  return true;
+}
+
+__device__ __forceinline__ bool ptc_wedge_or_rot(double* X, const double* E, const double* xe) {
+  if (xe[XE_GTOT] == 0) return ptc_rot_xz(X, E[XE_TANNA], E[XE_COSNA], E[XE_SINNA], xe);
+  return ptc_wedge(X, E, xe);
+}
+
+// ptc_fringe_dipoler, fringe_mod.f90:1151-1360 (b = E[XE_B]).  gfortran's
+// inline SUM starts from zero, kept for the sign of zero.
+__device__ __forceinline__ bool ptc_fringe_dipoler(double* X, const double* E, const double* xe) {
+  const double beta0 = xe[XE_BETA0], b = E[XE_B], fint = E[XE_FINT], hgap = E[XE_HGAP];
+  double fac = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[1] * X[1] - X[3] * X[3];
+  if (fac == 0) return false;
+  double pz = sqrt(fac);
+  double time_fac = xe[XE_IB] + X[4];
+  double xp = X[1] / pz, yp = X[3] / pz;
+  double d11 = (1.0 + xp * xp) / pz, d21 = xp * yp / pz, d31 = -xp;
+  double d12 = xp * yp / pz, d22 = (1.0 + yp * yp) / pz, d32 = -yp;
+  double d13 = -(time_fac * xp / (pz * pz)), d23 = -(time_fac * yp / (pz * pz)), d33 = time_fac / pz;
+  double u = 1.0 + yp * yp;
+  double w = 1.0 + (xp * xp) * (2.0 + yp * yp);
+  double fi0 = cr::atan(xp / u) - b * fint * hgap * 2.0 * w * pz;
+  double cf = cr::cos(fi0);
+  double co2 = b / (cf * cf);
+  double xu = xp / u;
+  double co1 = co2 / (1.0 + xu * xu);
+  double fi1 = co1 / u - co2 * b * fint * hgap * 2.0 * (2.0 * xp * (2.0 + yp * yp) * pz);
+  double fi2 = -(co1 * 2.0 * xp * yp / (u * u)) - co2 * b * fint * hgap * 2.0 * (2.0 * (xp * xp) * yp) * pz;
+  double fi3 = -(co2 * b * fint * hgap * 2.0 * w);
+  double fi0t = b * cr::tan(fi0);
+  double bb = 0.0 + fi1 * d12 + fi2 * d22 + fi3 * d32;
+  fac = 1.0 - 2.0 * bb * X[2];
+  if (fac < 0) return false;
+  X[2] = 2.0 * X[2] / (1.0 + sqrt(fac));
+  X[3] = X[3] - fi0t * X[2];
+  bb = 0.0 + fi1 * d11 + fi2 * d21 + fi3 * d31;
+  X[0] = X[0] + 0.5 * bb * (X[2] * X[2]);
+  bb = 0.0 + fi1 * d13 + fi2 * d23 + fi3 * d33;
+  X[5] = X[5] - 0.5 * bb * (X[2] * X[2]);
+  return true;
+}
+
+// exact_bend_edge_kick, fringe_mod.f90:1465-1577, with vec_bmad_to_ptc and
+// vec_ptc_to_bmad (:1599-1684): a failed step leaves the coordinates as they
+// were and the particle lost_pz.  Out of line (the particle passed and
+// returned by value), so that its temporaries do not raise the register
+// pressure of the element loop around it.
+template <bool ENTERING>
+BGT_DEV_NOINLINE Part exact_bend_edge(Part p, const double* xe) {
+  const double beta0 = xe[XE_BETA0], ib = xe[XE_IB];
+  const double* E = xe + (ENTERING ? XE_IN : XE_OUT);
+  const double v5 = p.z, v6 = p.pz;
+  double X[6];
+  X[0] = p.x;
+  X[1] = p.px;
+  X[2] = p.y;
+  X[3] = p.py;
+  X[4] = (v6 * v6 + 2 * v6) / (ib + sqrt(xe[XE_IB2] + v6 * v6 + 2 * v6));
+  X[5] = -(v5 * (ib + X[4]) / (1 + v6));
+  bool ok;
+  if (ENTERING) {
+    ok = ptc_rot_xz(X, E[XE_TANA], E[XE_COSA], E[XE_SINA], xe) && ptc_fringe_dipoler(X, E, xe) &&
+         ptc_wedge_or_rot(X, E, xe);
+  } else {
+    ok = ptc_wedge_or_rot(X, E, xe) && ptc_fringe_dipoler(X, E, xe) &&
+         ptc_rot_xz(X, E[XE_TANA], E[XE_COSA], E[XE_SINA], xe);
+  }
+  if (!ok) {
+    p.state = LOST_PZ;
+    return p;
+  }
+  double f1 = 1 + 2 * X[4] / beta0 + X[4] * X[4];
+  if (f1 <= 0) return p;
+  double t6 = (2 * X[4] / beta0 + X[4] * X[4]) / (sqrt(f1) + 1);
+  double t5 = -(X[5] * (1 + t6) / (ib + X[4]));
+  p.x = X[0];
+  p.px = X[1];
+  p.y = X[2];
+  p.py = X[3];
+  p.z = t5;
+  p.pz = t6;
+  return p;
 }
 
 // ---------------------------------------------------------------------------

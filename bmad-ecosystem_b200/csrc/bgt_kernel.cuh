@@ -562,10 +562,14 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
     else
       offset_set(p, R.mis, fl, G, m, true);
   }
-  const double* ext = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);  // soft / linear edge constants
+  const double* ext = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);  // soft / linear / exact edge constants
   if (fl & F_EDGE_IN) {
     // apply_element_edge_kick.f90:160-201: entering, magnetic (bend_edge_kick,
     // fringe_mod.f90:39-127) then electric
+    if (RARE && (fl & F_EXACT_EDGE)) {
+      hard_multipole_edge_kick<1>(p, ext[XE_K1], true);
+      p = exact_bend_edge<true>(p, ext);
+    }
     if (RARE && (fl & F_SOFT_EDGE)) sad_soft_bend_edge(p, ext, true);
     if (!(RARE && (fl & F_NO_HWANG))) hwang_edge<true>(p, q + B_EDGE);
     if (RARE && (fl & F_LINEAR_EDGE)) linear_bend_edge(p, ext, true);
@@ -645,6 +649,10 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
   if (fl & F_EDGE_OUT) {
     // leaving: electric then magnetic
     if (RARE && (fl & F_ELEC_EDGE)) electric_longitudinal_fringe(p, ae, be, ixe, -1.0, G);
+    if (RARE && (fl & F_EXACT_EDGE)) {
+      p = exact_bend_edge<false>(p, ext);
+      hard_multipole_edge_kick<1>(p, ext[XE_K1], false);
+    }
     if (RARE && (fl & F_LINEAR_EDGE)) linear_bend_edge(p, ext, false);
     if (!(RARE && (fl & F_NO_HWANG))) hwang_edge<false>(p, q + B_EDGE + EDGE_N);
     if (RARE && (fl & F_SOFT_EDGE)) sad_soft_bend_edge(p, ext, false);
@@ -778,9 +786,11 @@ constexpr int MAX_BLOCK = 256;
 //   memory to more resident CTAs; CTA-wide tiles as in TMODE 0.
 // TMODE 2: global-memory tables with every warp scheduled on its own.
 // RARE: the element loop also handles the rarely used record features --
-//   electric multipoles, the quadrupole/sextupole hard-edge multipole fringe
-//   and apertures checked in the element frame (F_FRINGE_INFO, F_ELEC,
-//   F_AP_OFFSET).  Lattices without them run the RARE = false kernel, whose
+//   electric multipoles, the quadrupole/sextupole hard-edge multipole fringe,
+//   apertures checked in the element frame, misaligned bends, RF couplers and
+//   the bend edges other than Hwang's (F_FRINGE_INFO, F_ELEC, F_AP_OFFSET,
+//   F_BEND_MIS, F_COUPLER_*, F_SOFT_EDGE, F_LINEAR_EDGE, F_EXACT_EDGE,
+//   F_NO_HWANG).  Lattices without them run the RARE = false kernel, whose
 //   element loop carries none of that code (a smaller instruction footprint
 //   and register budget for the common case); the host picks the variant
 //   from the compiled tables, never the other way round.

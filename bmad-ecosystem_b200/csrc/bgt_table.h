@@ -74,8 +74,12 @@ enum Flag : int32_t {
   // bend linear_edge fringe: ht_x, ht_y at the entrance, then at the exit,
   // after the electric multipoles
   F_LINEAR_EDGE = 1 << 25,
-  // bend edges without the Hwang map (soft_edge_only, linear_edge)
+  // bend edges without the Hwang map (soft_edge_only, linear_edge, full)
   F_NO_HWANG = 1 << 26,
+  // bend fringe_type full: the exact (PTC) bend edge and the k1 hard-edge
+  // multipole fringe, an exact-edge block (XE_*) after the electric
+  // multipoles
+  F_EXACT_EDGE = 1 << 27,
 };
 
 struct RecHdr {
@@ -168,6 +172,19 @@ constexpr int EDGE_GT = 0, EDGE_GT2 = 1, EDGE_GS2 = 2, EDGE_K1TANE = 3, EDGE_K1T
               EDGE_C1 = 6, EDGE_C3 = 7, EDGE_C4 = 8, EDGE_GPG = 9, EDGE_GTGS2_2K1 = 10;
 constexpr int EDGE_N = 11;
 constexpr int B_N = B_EDGE + 2 * EDGE_N;
+
+// Exact bend edge block (F_EXACT_EDGE, exact_bend_edge_kick,
+// fringe_mod.f90:1465-1686): beta0 = p0c / e_tot, 1 / beta0,
+// 1 / beta0**2, g_tot (0 for a bend that is off), k1 (hard-edge multipole
+// fringe), then one block per end, entrance first.  Per end, with a the
+// edge angle (e1 or e2): a, tan / cos / sin of a (the frame rotation),
+// -a, tan / cos / sin of -a and sin(-2a) (the wedge, or a rotation when
+// g_tot = 0), then the dipole fringe's b (g_tot at the entrance, -g_tot at
+// the exit), fint and hgap (fintx and hgapx at the exit).
+constexpr int XE_BETA0 = 0, XE_IB = 1, XE_IB2 = 2, XE_GTOT = 3, XE_K1 = 4, XE_IN = 5;
+constexpr int XE_A = 0, XE_TANA = 1, XE_COSA = 2, XE_SINA = 3, XE_NA = 4, XE_TANNA = 5, XE_COSNA = 6,
+              XE_SINNA = 7, XE_SIN2NA = 8, XE_B = 9, XE_FINT = 10, XE_HGAP = 11, XE_END_N = 12;
+constexpr int XE_OUT = XE_IN + XE_END_N, XE_N = XE_IN + 2 * XE_END_N;
 
 // Thin multipole: per pole n (0..ix_mag_max): knl, cos(tilt), sin(tilt), tilt_is_zero
 constexpr int TH_REFORB = 0;  // ref_orb_offset (1.0 for multipole$, else 0)

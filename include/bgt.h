@@ -44,10 +44,11 @@
  * Scope: forward tracking (direction = time_dir = orientation = +1), relative
  * RF time (bmad_com%absolute_time_tracking = F), magnetic and electric
  * multipoles (electric ones on quadrupoles, sextupoles, octupoles, thick
- * multipoles and bends), misaligned elements including bends, RF coupler
- * kicks, no radiation/spin, no exact bend multipoles, no full (exact) bend
- * fringe.  bgt_create rejects any element outside that scope with
- * BGT_EUNSUPPORTED and names the element.
+ * multipoles and bends), misaligned elements including bends, the bend
+ * edges of every fringe type (the exact PTC edge of fringe_type full
+ * included), RF coupler kicks, no radiation/spin, no exact bend multipoles.
+ * bgt_create rejects any element outside that scope with BGT_EUNSUPPORTED
+ * and names the element.
  */
 #ifndef BGT_H
 #define BGT_H

@@ -66,6 +66,8 @@ static double P_ATAN2(double y, double x) { return (double)atan2q((__float128)y,
 static double P_SINH(double x) { return (double)sinhq((__float128)x); }
 static double P_COSH(double x) { return (double)coshq((__float128)x); }
 static double P_EXP(double x) { return (double)expq((__float128)x); }
+static double P_TAN(double x) { return (double)tanq((__float128)x); }
+static double P_ATAN(double x) { return (double)atanq((__float128)x); }
 #else
 #define P_SIN sin
 #define P_COS cos
@@ -74,6 +76,8 @@ static double P_EXP(double x) { return (double)expq((__float128)x); }
 #define P_SINH sinh
 #define P_COSH cosh
 #define P_EXP exp
+#define P_TAN tan
+#define P_ATAN atan
 #endif
 
 /* x**m for integer m, as gfortran evaluates it (repeated squaring,
@@ -1505,7 +1509,7 @@ static bgo_cplx cadd(bgo_cplx a, bgo_cplx b) {
 
 static void hard_multipole_edge_kick(const bgo_ele* ele, int first_edge, bgo_coord* orb) {
   int n_max;
-  if (ele->key == BGO_QUADRUPOLE) n_max = 1;
+  if (ele->key == BGO_QUADRUPOLE || ele->key == BGO_SBEND) n_max = 1; /* fringe_mod.f90:737-738 */
   else if (ele->key == BGO_SEXTUPOLE) n_max = 2;
   else return;
   double x = orb->vec[0], y = orb->vec[2];
@@ -1518,7 +1522,7 @@ static void hard_multipole_edge_kick(const bgo_ele* ele, int first_edge, bgo_coo
     poly_n1 = poly;
     poly = cmul(poly, xy);
     double ap = 0, bp;
-    if (ele->key == BGO_QUADRUPOLE) {
+    if (ele->key == BGO_QUADRUPOLE || ele->key == BGO_SBEND) {
       bp = ele->k1;
     } else {
       bp = ele->k2;
@@ -1637,6 +1641,146 @@ static void soft_quadrupole_edge_kick(const bgo_ele* ele, int first_edge, bgo_co
   FL(40);
 }
 
+/* The exact (PTC) bend edge of fringe_type full: exact_bend_edge_kick,
+ * bmad/modules/fringe_mod.f90:1465-1686, tracking part, forward
+ * (time_dir = 1).  The particle goes to PTC's (x, px, y, py, pt, ct)
+ * coordinates, through a rotation of the frame by the edge angle, the
+ * dipole fringe map and the wedge of the bend field, and back.  Each step
+ * returns 0 where the reference sets err_flag (the particle is then lost_pz
+ * with its Bmad coordinates untouched). */
+
+/* ptc_rot_xz, fringe_mod.f90:1384-1441: rotation of the frame about y. */
+static int ptc_rot_xz(double a, double X[6], double beta0) {
+  double arg = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[1] * X[1] - X[3] * X[3];
+  if (arg < 0) return 0;
+  double pz = sqrt(arg);
+  double pt = 1.0 - X[1] * tan(a) / pz;
+  double x1 = X[0];
+  X[0] = x1 / cos(a) / pt;
+  X[1] = X[1] * cos(a) + sin(a) * pz;
+  X[2] = X[2] + X[3] * x1 * tan(a) / pz / pt;
+  X[5] = X[5] + x1 * tan(a) / pz / pt * (1.0 / beta0 + X[4]);
+  FL(30);
+  return 1;
+}
+
+/* ptc_wedger, fringe_mod.f90:1020-1123: a wedge of angle a of the bend
+ * field g_tot (a plain rotation when g_tot = 0). */
+static int ptc_wedger(double a, double g_tot, double beta0, double X[6]) {
+  double b1 = g_tot;
+  if (b1 == 0) return ptc_rot_xz(a, X, beta0);
+  double fac = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[1] * X[1] - X[3] * X[3];
+  if (fac < 0) return 0;
+  double radix = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[3] * X[3];
+  if (radix < 1e-10) return 0;
+  double pz = sqrt(fac), pt = sqrt(radix);
+  double Xn1, Xn2, Xn3, Xn6;
+  Xn2 = X[1] * cos(a) + (pz - b1 * X[0]) * sin(a);
+  radix = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - Xn2 * Xn2 - X[3] * X[3];
+  if (radix < 1e-10) return 0;
+  double pzs = sqrt(radix);
+  double sa = sin(a);
+  Xn1 = X[0] * cos(a) + (X[0] * X[1] * sin(2.0 * a) + (sa * sa) * (2.0 * X[0] * pz - b1 * (X[0] * X[0]))) /
+                            (pzs + pz * cos(a) - X[1] * sin(a));
+  Xn3 = (a + P_ASIN(X[1] / pt) - P_ASIN(Xn2 / pt)) / b1;
+  Xn6 = X[5] + Xn3 * (1.0 / beta0 + X[4]);
+  Xn3 = X[2] + X[3] * Xn3;
+  X[0] = Xn1;
+  X[1] = Xn2;
+  X[2] = Xn3;
+  X[5] = Xn6;
+  LM(2);
+  FL(60);
+  return 1;
+}
+
+/* ptc_fringe_dipoler, fringe_mod.f90:1151-1360: the dipole fringe with the
+ * field integral fint * hgap; b = g_tot at the entrance, -g_tot at the exit.
+ * gfortran's inline SUM starts from zero, kept here for the sign of zero. */
+static int ptc_fringe_dipoler(double X[6], double g_tot, double beta0, double fint, double hgap, int first_edge) {
+  double b = first_edge ? g_tot : -g_tot;
+  double fac = 1.0 + 2.0 * X[4] / beta0 + X[4] * X[4] - X[1] * X[1] - X[3] * X[3];
+  if (fac == 0) return 0;
+  double pz = sqrt(fac);
+  double time_fac = 1.0 / beta0 + X[4];
+  double xp = X[1] / pz, yp = X[3] / pz;
+  double d11 = (1.0 + xp * xp) / pz, d21 = xp * yp / pz, d31 = -xp;
+  double d12 = xp * yp / pz, d22 = (1.0 + yp * yp) / pz, d32 = -yp;
+  double d13 = -(time_fac * xp / (pz * pz)), d23 = -(time_fac * yp / (pz * pz)), d33 = time_fac / pz;
+  double u = 1.0 + yp * yp;
+  double w = 1.0 + (xp * xp) * (2.0 + yp * yp);
+  double fi0 = P_ATAN(xp / u) - b * fint * hgap * 2.0 * w * pz;
+  double cf = P_COS(fi0);
+  double co2 = b / (cf * cf);
+  double xu = xp / u;
+  double co1 = co2 / (1.0 + xu * xu);
+  double fi1 = co1 / u - co2 * b * fint * hgap * 2.0 * (2.0 * xp * (2.0 + yp * yp) * pz);
+  double fi2 = -(co1 * 2.0 * xp * yp / (u * u)) - co2 * b * fint * hgap * 2.0 * (2.0 * (xp * xp) * yp) * pz;
+  double fi3 = -(co2 * b * fint * hgap * 2.0 * w);
+  double fi0t = b * P_TAN(fi0);
+  double bb = 0.0 + fi1 * d12 + fi2 * d22 + fi3 * d32;
+  fac = 1.0 - 2.0 * bb * X[2];
+  if (fac < 0) return 0;
+  X[2] = 2.0 * X[2] / (1.0 + sqrt(fac));
+  X[3] = X[3] - fi0t * X[2];
+  bb = 0.0 + fi1 * d11 + fi2 * d21 + fi3 * d31;
+  X[0] = X[0] + 0.5 * bb * (X[2] * X[2]);
+  bb = 0.0 + fi1 * d13 + fi2 * d23 + fi3 * d33;
+  X[5] = X[5] - 0.5 * bb * (X[2] * X[2]);
+  LM(3);
+  FL(110);
+  return 1;
+}
+
+/* exact_bend_edge_kick, fringe_mod.f90:1465-1577, with vec_bmad_to_ptc and
+ * vec_ptc_to_bmad (:1599-1684).  orb%t is not tracked (relative RF time). */
+static void exact_bend_edge_kick(const bgo_ele* ele, int first_edge, bgo_coord* orb) {
+  double beta0 = ele->p0c / ele->e_tot;
+  double g_tot = ele->is_on ? ele->g + ele->dg : 0.0;
+  double X[6];
+  double v5 = orb->vec[4], v6 = orb->vec[5];
+  X[0] = orb->vec[0];
+  X[1] = orb->vec[1];
+  X[2] = orb->vec[2];
+  X[3] = orb->vec[3];
+  X[4] = (v6 * v6 + 2 * v6) / (1 / beta0 + sqrt(1 / (beta0 * beta0) + v6 * v6 + 2 * v6));
+  X[5] = -(v5 * (1 / beta0 + X[4]) / (1 + v6));
+  double edge_angle, fint, hgap;
+  if (first_edge) {
+    edge_angle = 1 * ele->e1;
+    fint = ele->fint;
+    hgap = ele->hgap;
+  } else {
+    edge_angle = 1 * ele->e2;
+    fint = ele->fintx;
+    hgap = ele->hgapx;
+  }
+  int ok;
+  if (first_edge) {
+    ok = ptc_wedger(edge_angle, 0.0, beta0, X) && ptc_fringe_dipoler(X, g_tot, beta0, 1 * fint, hgap, 1) &&
+         ptc_wedger(-edge_angle, g_tot, beta0, X);
+  } else {
+    ok = ptc_wedger(-edge_angle, g_tot, beta0, X) && ptc_fringe_dipoler(X, g_tot, beta0, 1 * fint, hgap, 0) &&
+         ptc_wedger(edge_angle, 0.0, beta0, X);
+  }
+  FL(20);
+  if (!ok) {
+    orb->state = BGO_LOST_PZ;
+    return;
+  }
+  double f1 = 1 + 2 * X[4] / beta0 + X[4] * X[4];
+  if (f1 <= 0) return;
+  double t6 = (2 * X[4] / beta0 + X[4] * X[4]) / (sqrt(f1) + 1);
+  double t5 = -(X[5] * (1 + t6) / (1 / beta0 + X[4]));
+  orb->vec[0] = X[0];
+  orb->vec[1] = X[1];
+  orb->vec[2] = X[2];
+  orb->vec[3] = X[3];
+  orb->vec[4] = t5;
+  orb->vec[5] = t6;
+  FL(12);
+}
+
 static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first_edge, const bgo_param* param,
                                    const double* ae, const double* be, int ix_elec_max) {
   int physical_end = first_edge ? BGO_ENTRANCE_END : BGO_EXIT_END;
@@ -1662,8 +1806,7 @@ static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first
       break;
     }
     case BGO_SBEND:
-      /* bend_edge_kick, fringe_mod.f90:39-127: fringe_here, hard multipole edge
-       * (only for fringe_type full: not restated), then Hwang. */
+      /* bend_edge_kick, fringe_mod.f90:39-127 */
       if (ele->fringe_type == BGO_FRINGE_NONE) break;
       if (ele->fringe_type == BGO_FRINGE_BASIC_BEND || ele->fringe_type == BGO_FRINGE_HARD_EDGE_ONLY) {
         bgo_hwang_bend_edge_kick(ele, first_edge, orb, param);
@@ -1680,7 +1823,11 @@ static int apply_element_edge_kick(bgo_coord* orb, const bgo_ele* ele, int first
       } else if (ele->fringe_type == BGO_FRINGE_LINEAR_EDGE) {
         linear_bend_edge_kick(ele, first_edge, orb);
       } else {
-        return -1; /* full: the exact (PTC) bend edge is not restated */
+        /* full: the k1 hard-edge multipole fringe (fringe_mod.f90:63-65,
+         * 102-104) around the exact edge */
+        if (first_edge) hard_multipole_edge_kick(ele, first_edge, orb);
+        exact_bend_edge_kick(ele, first_edge, orb);
+        if (!first_edge) hard_multipole_edge_kick(ele, first_edge, orb);
       }
       break;
     default:

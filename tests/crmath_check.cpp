@@ -1,4 +1,4 @@
-// Host check of the device's correctly rounded sin/cos/sinh/cosh/exp/asin/atan2
+// Host check of the device's correctly rounded sin/cos/tan/sinh/cosh/exp/asin/atan/atan2
 // (bmad-ecosystem_b200/csrc/bgt_crmath.cuh, compiled here for the CPU)
 // against libquadmath evaluated in binary128 and rounded to double.
 //
@@ -42,6 +42,8 @@ static double cr_eval(const char* fn, double x, double y) {
   if (!strcmp(fn, "cosh")) return bgt::cr::cosh(x);
   if (!strcmp(fn, "asin")) return bgt::cr::asin(x);
   if (!strcmp(fn, "exp")) return bgt::cr::exp(x);
+  if (!strcmp(fn, "tan")) return bgt::cr::tan(x);
+  if (!strcmp(fn, "atan")) return bgt::cr::atan(x);
   return bgt::cr::atan2(y, x);
 }
 static double q_eval(const char* fn, double x, double y) {
@@ -52,6 +54,8 @@ static double q_eval(const char* fn, double x, double y) {
   else if (!strcmp(fn, "cosh")) q = coshq(x);
   else if (!strcmp(fn, "asin")) q = asinq(x);
   else if (!strcmp(fn, "exp")) q = expq(x);
+  else if (!strcmp(fn, "tan")) q = tanq(x);
+  else if (!strcmp(fn, "atan")) q = atanq(x);
   else q = atan2q(y, x);
   return (double)q;
 }
@@ -72,6 +76,8 @@ int main(int argc, char** argv) {
       {"sin", -0.78, 0.78, 0}, {"sin", -30.0, 30.0, 0}, {"cos", -0.78, 0.78, 0}, {"cos", -30.0, 30.0, 0},
       {"sinh", -2.0, 2.0, 0}, {"cosh", -2.0, 2.0, 0}, {"exp", -2.0, 2.0, 0}, {"asin", -1.0, 1.0, 0},
       {"atan2", -4.0, 4.0, 0},
+      {"tan", 0x1p-30, 0x1p-4, 1}, {"tan", -1.5, 1.5, 0}, {"tan", -30.0, 30.0, 0},
+      {"atan", 0x1p-30, 0x1p-4, 1}, {"atan", -4.0, 4.0, 0}, {"atan", -1e3, 1e3, 0},
   };
   long total_bad = 0;
   for (const Range& r : rs) {

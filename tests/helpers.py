@@ -84,8 +84,9 @@ def rare_zoo_lattice() -> L.Lattice:
     bends (offset_particle's bend geometry, with g, ref_tilt or roll), the
     straight geometry of a misaligned g = 0 bend, electric multipoles in bends
     and quadrupoles, the hard-edge multipole fringe, the soft-edge quadrupole
-    fringe, the SAD soft and linear bend edges, an RF coupler kick and a
-    misaligned collimator whose aperture moves with it -- at the 5 GeV ring
+    fringe, the SAD soft and linear bend edges, an RF coupler kick, a
+    misaligned collimator whose aperture moves with it and the exact bend
+    edge of fringe_type full (with g + dg = 0 too) -- at the 5 GeV ring
     energy."""
     E = []
     E.append(L.Element("drift", "D", {"l": 0.5}))
@@ -118,6 +119,15 @@ def rare_zoo_lattice() -> L.Lattice:
                        num_steps=6, coupler_at="both_ends"))
     E.append(L.Element("ecollimator", "ECMIS", {"l": 0.2, "x1_limit": 0.015, "x2_limit": 0.0165, "y1_limit": 0.01,
                                                 "y2_limit": 0.01, "x_offset": 5e-4, "tilt": 0.2}))
+    # fringe_type full: the exact (PTC) bend edge inside the k1 hard-edge fringe
+    E.append(L.Element("sbend", "BFULL", {"l": 1.0, "g": 0.02, "k1": 0.05, "e1": 0.06, "e2": 0.03, "fint": 0.5,
+                                          "hgap": 0.03}, fringe_type="full"))
+    E.append(L.Element("sbend", "BFULLMIS", {"l": 0.6, "g": 0.01, "e1": 0.1, "e2": 0.2, "fint": 0.7, "hgap": 0.05,
+                                             "x_offset": 2e-4, "y_pitch": 1e-4, "ref_tilt": 0.1, "vkick": -1e-5,
+                                             "r0_mag": 2.0, "r0_elec": 3.0}, num_steps=10, fringe_type="full",
+                       a_pole={0: 1e-4, 1: 1e-3}, a_pole_elec={1: 2e6}, b_pole_elec={0: -2e5}))
+    E.append(L.Element("sbend", "BFULLG0", {"l": 0.5, "k1": 0.08, "e1": 0.05, "e2": -0.04, "fint": 0.4,
+                                            "hgap": 0.02}, fringe_type="full"))
     lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "rare_zoo")
     return lat.finalize()
 

@@ -90,14 +90,22 @@ ELEMENTS = {
     "RFCAVITY3": ("rfcavity", {"rf_frequency": 500e6, "voltage": 1e5, "phi0": 0.1, "x_offset": 0.05,
                                "y_pitch": 0.001, "tilt": 0.1}, {"num_steps": 10, "a_pole": {2: 0.02}}),
 }
-# tracking_method_test.bmad:84,89-91 (the rows without exact multipoles or a
-# full bend fringe): misaligned bends with ref_tilt, electric multipoles
-for _n, _key, _b in (("SBEND3", "sbend", sb0(l=0.6, k1=0.3, k2=3.0, x_offset=0.05, y_pitch=0.001, ref_tilt=0.1)),
-                     ("RBEND6", "rbend", sb0(l=0.6, g=0.01, dg=-0.0099999, e1=0.1, e2=0.2, x_offset=0.05,
-                                             y_pitch=0.001, ref_tilt=0.1)),
-                     ("SBEND7", "sbend", sb0(l=0.6, g=0.01, e1=0.1, e2=0.2, x_offset=0.05, y_pitch=0.001,
-                                             ref_tilt=0.1))):
+# tracking_method_test.bmad:84-91 (the rows without exact multipoles):
+# misaligned bends with ref_tilt, electric multipoles; RBEND4 and SBEND5 with
+# the exact (PTC) bend edge of fringe_type full
+for _n, _key, _b, _fr in (
+        ("SBEND3", "sbend", sb0(l=0.6, k1=0.3, k2=3.0, x_offset=0.05, y_pitch=0.001, ref_tilt=0.1), None),
+        ("RBEND4", "rbend", sb0(l=0.6, g=0.01, dg=-0.0099, e1=0.1, e2=0.2, x_offset=0.05, y_pitch=0.001,
+                                ref_tilt=0.1), "full"),
+        ("SBEND5", "sbend", sb0(l=0.6, g=0.01, e1=0.1, e2=0.2, x_offset=0.05, y_pitch=0.001, ref_tilt=0.1,
+                                fint=0.7, hgap=2.0), "full"),
+        ("RBEND6", "rbend", sb0(l=0.6, g=0.01, dg=-0.0099999, e1=0.1, e2=0.2, x_offset=0.05, y_pitch=0.001,
+                                ref_tilt=0.1), None),
+        ("SBEND7", "sbend", sb0(l=0.6, g=0.01, e1=0.1, e2=0.2, x_offset=0.05, y_pitch=0.001, ref_tilt=0.1),
+         None)):
     _kw = dict(num_steps=10, **_b)
+    if _fr:
+        _kw["fringe_type"] = _fr
     ELEMENTS[_n] = (_key, _kw.pop("values"), _kw)
 for _n, _k1, _fr in (("QUADRUPOLE1", 1.0, None), ("QUADRUPOLE2", -1.0, None), ("QUADRUPOLE3", 1e-20, None),
                      ("QUADRUPOLE4", 1.0, "full"), ("QUADRUPOLE5", -1.0, "full")):
