@@ -598,10 +598,6 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
         err = ename(e) + ": bend fringe_type " + std::to_string(ft) + " is not supported";
         return BGT_EUNSUPPORTED;
       }
-      if (ixe > -1 && !edges && e.fringe_at != BGT_NO_END) {
-        err = ename(e) + ": electric multipoles on a bend with fringe_type none are not supported";
-        return BGT_EUNSUPPORTED;
-      }
       // multipole_ele_to_ab(..., include_kicks$, b1) then track_a_bend.f90:58-94
       double b1 = bn[1];
       bn[1] = 0;
@@ -658,10 +654,14 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       q[B_K1 + 0] = b1 / e.l;
       q[B_K1 + 1] = 1 * e.l / n_step;
       q[B_K1 + 2] = g_tot;
-      if (edges) {
+      // the ends act for a fringe type or for the electric longitudinal
+      // fringe alone (fringe_type none with electric multipoles:
+      // apply_element_edge_kick.f90:101-103, 152-153)
+      if (edges || ixe > -1) {
         if (e.fringe_at == BGT_ENTRANCE_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_IN;
         if (e.fringe_at == BGT_EXIT_END || e.fringe_at == BGT_BOTH_ENDS) flags |= F_EDGE_OUT;
       }
+      if (!edges && ixe > -1) flags |= F_NO_HWANG;
       put_edge(q + B_EDGE, e, true);
       put_edge(q + B_EDGE + EDGE_N, e, false);
       // bend_edge_kick (fringe_mod.f90:39-127): the Hwang map for basic_bend,

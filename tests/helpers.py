@@ -128,6 +128,10 @@ def rare_zoo_lattice() -> L.Lattice:
                        a_pole={0: 1e-4, 1: 1e-3}, a_pole_elec={1: 2e6}, b_pole_elec={0: -2e5}))
     E.append(L.Element("sbend", "BFULLG0", {"l": 0.5, "k1": 0.08, "e1": 0.05, "e2": -0.04, "fint": 0.4,
                                             "hgap": 0.02}, fringe_type="full"))
+    # fringe_type none with electric multipoles: the electric longitudinal
+    # fringe alone at the ends
+    E.append(L.Element("sbend", "BELECNONE", {"l": 0.7, "g": 0.012, "e1": 0.04}, fringe_type="none",
+                       b_pole_elec={0: 1e4, 2: 3e7}))
     lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "rare_zoo")
     return lat.finalize()
 
