@@ -31,7 +31,10 @@ class BgtElement(C.Structure):
             "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",
             "x1_limit", "x2_limit", "y1_limit", "y2_limit")] + [
         (n, C.c_double * N_POLE) for n in ("an", "bn", "an_elec", "bn_elec", "knl", "tn")] + [
-        ("coupler_angle", C.c_double), ("coupler_phase", C.c_double), ("fq1", C.c_double), ("fq2", C.c_double)]
+        ("coupler_angle", C.c_double), ("coupler_phase", C.c_double), ("fq1", C.c_double), ("fq2", C.c_double)] + [
+        (n, C.c_double) for n in ("px_aperture_width2", "px_aperture_center", "py_aperture_width2",
+                                  "py_aperture_center", "z_aperture_width2", "z_aperture_center",
+                                  "pz_aperture_width2", "pz_aperture_center")]
 
 
 class BgtSpecies(C.Structure):
@@ -124,7 +127,9 @@ def to_bgt_element(e: L.Element) -> BgtElement:
     for n in ("l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", "hgapx", "voltage", "phi0",
               "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset",
               "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",
-              "x1_limit", "x2_limit", "y1_limit", "y2_limit"):
+              "x1_limit", "x2_limit", "y1_limit", "y2_limit", "px_aperture_width2", "px_aperture_center",
+              "py_aperture_width2", "py_aperture_center", "z_aperture_width2", "z_aperture_center",
+              "pz_aperture_width2", "pz_aperture_center"):
         setattr(b, n, e.v(n))
     if e.key in ("multipole", "ab_multipole"):
         _, knl, tn = L.multipole_ele_to_kt(e, True)

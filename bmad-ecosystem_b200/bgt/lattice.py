@@ -62,6 +62,8 @@ _VALUE_NAMES = [
     "phi0_multipass", "rf_frequency", "coupler_strength", "p0c", "e_tot", "ds_step", "x_offset", "y_offset",
     "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick", "x1_limit",
     "x2_limit", "y1_limit", "y2_limit", "r0_mag", "r0_elec", "coupler_angle", "coupler_phase", "fq1", "fq2",
+    "px_aperture_width2", "px_aperture_center", "py_aperture_width2", "py_aperture_center", "z_aperture_width2",
+    "z_aperture_center", "pz_aperture_width2", "pz_aperture_center",
 ]
 
 

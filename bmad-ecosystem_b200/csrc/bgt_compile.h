@@ -418,6 +418,22 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     if (e.aperture_at == BGT_EXIT_END || e.aperture_at == BGT_BOTH_ENDS) flags |= F_AP_EXIT;
     flags |= ap_ell ? F_AP_ELLIPTICAL : F_AP_RECT;
   }
+  // a collimator's momentum and longitudinal limits (check_aperture_limit.f90:
+  // 98-135) are checked at the ends aperture_at names whatever the transverse
+  // limits; without transverse limits the aperture block holds zeros (no
+  // transverse check)
+  const bool ap_mom = (key == BGT_ECOLLIMATOR || key == BGT_RCOLLIMATOR) && e.aperture_at != BGT_NO_END &&
+                      (e.px_aperture_width2 != 0 || e.py_aperture_width2 != 0 || e.z_aperture_width2 != 0 ||
+                       e.pz_aperture_width2 != 0);
+  if (ap_mom) {
+    if (!ap_any) {
+      if (e.aperture_at == BGT_ENTRANCE_END || e.aperture_at == BGT_BOTH_ENDS) flags |= F_AP_ENTRANCE;
+      if (e.aperture_at == BGT_EXIT_END || e.aperture_at == BGT_BOTH_ENDS) flags |= F_AP_EXIT;
+      flags |= F_AP_RECT;
+    }
+    flags |= F_AP_MOMENTUM;
+    if (key == BGT_ECOLLIMATOR) flags |= F_AP_MOM_ELL;
+  }
 
   if (flags & F_MISALIGN) {
     double* m = B.ptr_after_push(MIS_N);
@@ -452,11 +468,11 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
   }
   if (flags & (F_AP_ENTRANCE | F_AP_EXIT)) {
     double* a = B.ptr_after_push(AP_N);
-    a[AP_X1] = -e.x1_limit;
-    a[AP_X2] = e.x2_limit;
-    a[AP_Y1] = -e.y1_limit;
-    a[AP_Y2] = e.y2_limit;
-    if (ap_ell) {
+    a[AP_X1] = ap_any ? -e.x1_limit : 0.0;
+    a[AP_X2] = ap_any ? e.x2_limit : 0.0;
+    a[AP_Y1] = ap_any ? -e.y1_limit : 0.0;
+    a[AP_Y2] = ap_any ? e.y2_limit : 0.0;
+    if (ap_any && ap_ell) {
       double w = (a[AP_X2] - a[AP_X1]) / 2, c = (a[AP_X2] + a[AP_X1]) / 2;
       if (w == 0) w = sp.max_aperture_limit;
       a[AP_XW] = std::max(w, 0.0);
@@ -466,6 +482,17 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       if (w == 0) w = sp.max_aperture_limit;
       a[AP_YW] = std::max(w, 0.0);
       a[AP_YC] = c;
+    }
+    if (flags & F_AP_MOMENTUM) {
+      double* m = B.ptr_after_push(APM_N);
+      m[APM_PXW] = e.px_aperture_width2;
+      m[APM_PXC] = e.px_aperture_center;
+      m[APM_PYW] = e.py_aperture_width2;
+      m[APM_PYC] = e.py_aperture_center;
+      m[APM_ZW] = e.z_aperture_width2;
+      m[APM_ZC] = e.z_aperture_center;
+      m[APM_PZW] = e.pz_aperture_width2;
+      m[APM_PZC] = e.pz_aperture_center;
     }
   }
 
@@ -835,7 +862,7 @@ static void c_multi_tables(double cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1],
 // Whether a compiled record uses a feature only the RARE kernels handle.
 static bool record_is_rare(const RecHdr* rh) {
   return (rh->flags & (F_FRINGE_INFO | F_ELEC | F_AP_OFFSET | F_BEND_MIS | F_COUPLER_IN | F_COUPLER_OUT |
-                       F_SOFT_EDGE | F_LINEAR_EDGE | F_NO_HWANG | F_EXACT_EDGE)) != 0;
+                       F_SOFT_EDGE | F_LINEAR_EDGE | F_NO_HWANG | F_EXACT_EDGE | F_AP_MOMENTUM)) != 0;
 }
 
 // The element tables of all variants, as bgt_create uploads them.  Per

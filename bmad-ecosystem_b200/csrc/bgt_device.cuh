@@ -166,7 +166,11 @@ __device__ __forceinline__ void aperture_frame(const Part& p, const double* mis,
   }
 }
 
-__device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32_t flags, double px_, double py_) {
+// UF: the unstable factor starts from uf0 (a collimator's momentum limits
+// went first) instead of 0.
+template <bool UF = false>
+__device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32_t flags, double px_, double py_,
+                                                double uf0 = 0.0) {
   if (flags & F_AP_ELLIPTICAL) {
     double xp = px_ - ap[AP_XC];
     double yp = py_ - ap[AP_YC];
@@ -178,7 +182,7 @@ __device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32
       p.state = yp > 0 ? LOST_POS_Y : LOST_NEG_Y;
     }
   } else {
-    double uf = 0, f;
+    double uf = UF ? uf0 : 0, f;
     const double x1 = ap[AP_X1], x2 = ap[AP_X2], y1 = ap[AP_Y1], y2 = ap[AP_Y2];
     const double xv = px_, yv = py_;
     if (x1 != 0 && xv < x1) {
@@ -212,11 +216,49 @@ __device__ __forceinline__ void aperture_limits(Part& p, const double* ap, int32
   }
 }
 
+// check_this_limit, check_aperture_limit.f90:329-341
+__device__ __forceinline__ void check_this_limit(Part& p, double coord, double width2, double center, double& uf) {
+  if (width2 == 0) return;
+  if (coord > center - width2 && coord < center + width2) return;
+  p.state = LOST;
+  uf = fmax((center - width2) - coord, coord - (center + width2));
+}
+
+// A collimator's momentum and longitudinal limits, check_aperture_limit.f90:
+// 98-135, on the lab-frame coordinates: the ecollimator's (px, py) and
+// (z, pz) pairs are ellipses when both widths are set, the rcollimator's four
+// limits independent.
+__device__ __forceinline__ void collimator_momentum_limits(Part& p, const double* m, int32_t flags, double& uf) {
+  if (flags & F_AP_MOM_ELL) {
+    for (int k = 0; k < 2; k++) {
+      const double xw2 = m[4 * k + 0], x0 = m[4 * k + 1], yw2 = m[4 * k + 2], y0 = m[4 * k + 3];
+      const double u = k == 0 ? p.px : p.z, v = k == 0 ? p.py : p.pz;
+      if (xw2 == 0 || yw2 == 0) {
+        check_this_limit(p, u, xw2, x0, uf);
+        check_this_limit(p, v, yw2, y0, uf);
+      } else {
+        const double r = sq((u - x0) / xw2) + sq((v - y0) / yw2);
+        if (r > 1) {
+          p.state = LOST;
+          uf = sqrt(r) - 1;
+        }
+      }
+    }
+  } else {
+    check_this_limit(p, p.px, m[APM_PXW], m[APM_PXC], uf);
+    check_this_limit(p, p.py, m[APM_PYW], m[APM_PYC], uf);
+    check_this_limit(p, p.z, m[APM_ZW], m[APM_ZC], uf);
+    check_this_limit(p, p.pz, m[APM_PZW], m[APM_PZC], uf);
+  }
+}
+
 __device__ __forceinline__ void check_aperture(Part& p, const double* ap, const double* mis, int32_t flags,
                                                bool at_exit) {
   double xa, ya;
+  double uf = 0;
+  if (flags & F_AP_MOMENTUM) collimator_momentum_limits(p, ap + AP_N, flags, uf);
   aperture_frame(p, mis, flags, at_exit, xa, ya);
-  aperture_limits(p, ap, flags, xa, ya);
+  aperture_limits<true>(p, ap, flags, xa, ya, uf);
 }
 
 // ---------------------------------------------------------------------------

@@ -57,6 +57,7 @@ __device__ __forceinline__ Rec decode(const double* r) {
   if (fl & (F_AP_ENTRANCE | F_AP_EXIT)) {
     R.ap = q;
     q += AP_N;
+    if (RARE && (fl & F_AP_MOMENTUM)) q += APM_N;  // collimator momentum limits follow
   }
   R.kb = q;
   return R;

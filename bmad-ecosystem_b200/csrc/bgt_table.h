@@ -80,6 +80,11 @@ enum Flag : int32_t {
   // multipole fringe, an exact-edge block (XE_*) after the electric
   // multipoles
   F_EXACT_EDGE = 1 << 27,
+  // collimator momentum / longitudinal limits (check_aperture_limit.f90:
+  // 98-135), a block of APM_N doubles after the aperture block;
+  // F_AP_MOM_ELL: the ecollimator's elliptical pairs
+  F_AP_MOMENTUM = 1 << 28,
+  F_AP_MOM_ELL = 1 << 29,
 };
 
 struct RecHdr {
@@ -134,6 +139,9 @@ constexpr int BM_N = BM_OPS_UNSET + BM_MAX_OPS * BM_OP_N;
 constexpr int AP_X1 = 0, AP_X2 = 1, AP_Y1 = 2, AP_Y2 = 3;  // x1_lim = -x1_limit, ...
 constexpr int AP_XW = 4, AP_XC = 5, AP_YW = 6, AP_YC = 7;  // elliptical width2/center
 constexpr int AP_N = 8;
+// Collimator momentum block (F_AP_MOMENTUM): width2 and center of px, py, z, pz
+constexpr int APM_PXW = 0, APM_PXC = 1, APM_PYW = 2, APM_PYC = 3, APM_ZW = 4, APM_ZC = 5, APM_PZW = 6,
+              APM_PZC = 7, APM_N = 8;
 
 // Drift: L
 constexpr int DR_L = 0, DR_N = 1;

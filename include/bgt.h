@@ -134,6 +134,10 @@ typedef struct bgt_element {
   double knl[BGT_N_POLE], tn[BGT_N_POLE];
   double coupler_angle, coupler_phase; /* rfcavity coupler (with coupler_strength) */
   double fq1, fq2;                     /* quadrupole soft-edge fringe integrals */
+  /* ecollimator / rcollimator momentum and longitudinal limits
+   * (check_aperture_limit.f90:98-135); width2 = 0: no limit */
+  double px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center;
+  double z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center;
 } bgt_element;
 
 /* Tracked species (lat%param%particle) and bmad_com switches. */

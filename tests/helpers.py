@@ -132,6 +132,14 @@ def rare_zoo_lattice() -> L.Lattice:
     # fringe alone at the ends
     E.append(L.Element("sbend", "BELECNONE", {"l": 0.7, "g": 0.012, "e1": 0.04}, fringe_type="none",
                        b_pole_elec={0: 1e4, 2: 3e7}))
+    # collimator momentum and longitudinal limits: the ecollimator's (px, py)
+    # ellipse and a single z limit, an rcollimator with no transverse limits
+    E.append(L.Element("ecollimator", "ECMOM", {"l": 0.1, "x1_limit": 0.03, "x2_limit": 0.03, "y1_limit": 0.02,
+                                                "y2_limit": 0.02, "px_aperture_width2": 1.2e-3,
+                                                "py_aperture_width2": 6e-4, "px_aperture_center": 1e-4,
+                                                "z_aperture_width2": 0.013}))
+    E.append(L.Element("rcollimator", "RCMOM", {"l": 0.1, "pz_aperture_width2": 0.011, "pz_aperture_center": 5e-4,
+                                                "py_aperture_width2": 7e-4}))
     lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "rare_zoo")
     return lat.finalize()
 

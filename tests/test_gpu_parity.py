@@ -96,8 +96,8 @@ def test_rare_zoo_each_element_bitwise(rare_zoo):
 def test_rare_zoo_turns_with_losses(rare_zoo):
     lat, tr = rare_zoo
     # the line does not close, so the orbit grows turn by turn: particles are
-    # lost at the collimator over all five turns
-    v0 = random_particles(4096, seed=22)
+    # lost at the collimators over all five turns
+    v0 = random_particles(4096, seed=22, scale=0.1)
     b = tr.make_bunch(v0.copy())
     tr.track_turns(b, 5)
     ov, ob, ost, oie, oit = oracle_track_elements(lat, v0, 0, len(lat), 5, variant="cr")
