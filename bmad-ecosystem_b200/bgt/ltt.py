@@ -1,4 +1,4 @@
-"""long_term_tracking's BEAM-mode turn loop on the tracker.
+"""long_term_tracking's BEAM-mode and single-particle turn loops on the tracker.
 
 Restates ``ltt_run_beam_mode`` (bsim/modules/lt_tracking_mod.f90:1571-1719)
 for one bunch: the outputs at the start turn, the per-turn bookkeeping of
@@ -102,4 +102,70 @@ def run_beam_mode(tracker, bunch, ix_start_turn: int, ix_end_turn: int, dead_cut
         turn = stop_at
         res.ix_turn = turn
         emit(turn)
+    return res
+
+
+@dataclass
+class SingleModeResult:
+    ix_turn: np.ndarray  # per particle: the turn after its last tracked turn (the loss turn + 1 when lost)
+    rows: List[Tuple[int, int, np.ndarray]]  # (turn, particle, vec6) phase-space output rows
+    n_sum: np.ndarray  # per particle: turns summed into the averages
+    average: Optional[np.ndarray] = None  # [n, 6]: mean of vec over the summed turns
+    sigma: Optional[np.ndarray] = None  # [n, 6, 6]: <vec vec^T> - average average^T
+
+
+def run_single_mode(tracker, bunch, ix_turn_start: int, ix_turn_stop: int, particle_output_every_n_turns: int = 0,
+                    output_only_last_turns: int = -1, n_turns: Optional[int] = None,
+                    averages: bool = False) -> SingleModeResult:
+    """The single-particle turn loop ``ltt_run_single_mode``
+    (bsim/modules/lt_tracking_mod.f90:1333-1465) for every particle of
+    `bunch` at once -- the particles are independent, so one call per turn
+    (or per output interval) tracks them all, each stopping at its own loss.
+    Per particle: an output row at the start turn and after every turn that
+    is a multiple of `particle_output_every_n_turns` (while ``n_turns -
+    i_turn > output_only_last_turns`` or that bound is below 1, as the
+    reference tests it), nothing after the particle is lost; with `averages`
+    the mean and the second moments of vec over the turns survived
+    (ltt_write_single_mode_sigma_file, :2714-2749)."""
+    n = bunch.vec6.shape[1]
+    n_turns = (ix_turn_stop - ix_turn_start) if n_turns is None else n_turns
+    every = particle_output_every_n_turns
+    res = SingleModeResult(np.full(n, ix_turn_start, np.int64), [], np.zeros(n, np.int64))
+    acc = np.zeros((n, 6)) if averages else None
+    acc2 = np.zeros((n, 6, 6)) if averages else None
+    alive = bunch.state == L.ALIVE
+    for i in np.nonzero(alive)[0]:
+        res.rows.append((ix_turn_start, int(i), bunch.vec6[:, i].copy()))
+    turn = ix_turn_start
+    while turn < ix_turn_stop and np.any(bunch.state == L.ALIVE):
+        # without averages only the output turns need the coordinates
+        stop_at = turn + 1
+        if not averages:
+            stop_at = ix_turn_stop
+            if every > 0:
+                stop_at = min(stop_at, (turn // every + 1) * every)
+        alive0 = bunch.state == L.ALIVE
+        tracker.track_turns(bunch, stop_at - turn, turn0=turn)
+        alive1 = bunch.state == L.ALIVE
+        lost = alive0 & ~alive1
+        res.ix_turn[lost] = bunch.ix_turn_lost[lost] + 1
+        res.ix_turn[alive1] = stop_at
+        t = stop_at - 1  # the last turn of the segment
+        if averages:
+            v = bunch.vec6[:, alive1].T
+            acc[alive1] += v
+            acc2[alive1] += v[:, :, None] * v[:, None, :]
+            res.n_sum[alive1] += 1
+        do_write = output_only_last_turns < 1 or n_turns - t > output_only_last_turns
+        if every > 0 and do_write and (t + 1) % every == 0:
+            for i in np.nonzero(alive1)[0]:
+                res.rows.append((t + 1, int(i), bunch.vec6[:, i].copy()))
+        turn = stop_at
+    if averages:
+        ok = res.n_sum > 0
+        res.average = np.zeros((n, 6))
+        res.sigma = np.zeros((n, 6, 6))
+        res.average[ok] = acc[ok] / res.n_sum[ok, None]
+        res.sigma[ok] = acc2[ok] / res.n_sum[ok, None, None] - \
+            res.average[ok][:, :, None] * res.average[ok][:, None, :]
     return res

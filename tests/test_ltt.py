@@ -115,3 +115,52 @@ def test_resumed_start_turn_has_no_start_output(setup):
     b = Bunch.from_vec(v0.copy() * 0.1, lat.p0c, lat.species.mass)
     r = ltt.run_beam_mode(OracleTracker(lat, lib), b, 10, 16, outputs=[(2, lambda t, b_: seen.append(t))])
     assert seen == [12, 14, 16] and r.ix_turn == 16 and r.stop == "end_turn"
+
+
+def reference_single(tracker, lat, vec, start, stop, every, only_last, averages):
+    """ltt_run_single_mode for one particle, turn by turn
+    (lt_tracking_mod.f90:1394-1450)."""
+    b = Bunch.from_vec(vec.reshape(6, 1).copy(), lat.p0c, lat.species.mass)
+    rows = [(start, b.vec6[:, 0].copy())]
+    avg, sig, n_sum = np.zeros(6), np.zeros((6, 6)), 0
+    n_turns = stop - start
+    t_end = start
+    for t in range(start, stop):
+        tracker.track_turns(b, 1, turn0=t)
+        t_end = t + 1
+        if b.state[0] != L.ALIVE:
+            break
+        do_write = only_last < 1 or n_turns - t > only_last
+        if every > 0 and do_write and (t + 1) % every == 0:
+            rows.append((t + 1, b.vec6[:, 0].copy()))
+        if averages:
+            avg = avg + b.vec6[:, 0]
+            sig = sig + np.outer(b.vec6[:, 0], b.vec6[:, 0])
+            n_sum += 1
+    if averages and n_sum:
+        avg = avg / n_sum
+        sig = sig / n_sum - np.outer(avg, avg)
+    return t_end, rows, n_sum, avg, sig, b
+
+
+@pytest.mark.parametrize("every,only_last,averages", [(3, -1, False), (1, 5, True), (0, -1, True), (4, -1, True)])
+def test_single_mode_equals_one_particle_at_a_time(setup, every, only_last, averages):
+    lat, v0, lib = setup
+    idx = np.arange(0, 300, 15)  # 20 particles, several lost over the 20 turns
+    v = v0[:, idx].copy()
+    b = Bunch.from_vec(v.copy(), lat.p0c, lat.species.mass)
+    r = ltt.run_single_mode(OracleTracker(lat, lib), b, 2, 22, every, only_last, averages=averages)
+    n_lost = 0
+    for k in range(v.shape[1]):
+        t_end, rows, n_sum, avg, sig, bk = reference_single(OracleTracker(lat, lib), lat, v[:, k], 2, 22, every,
+                                                             only_last, averages)
+        n_lost += int(bk.state[0] != L.ALIVE)
+        assert r.ix_turn[k] == t_end
+        mine = [(t, vec) for t, i, vec in r.rows if i == k]
+        assert [t for t, _ in mine] == [t for t, _ in rows]
+        assert all(np.array_equal(a, c) for (_, a), (_, c) in zip(mine, rows))
+        assert np.array_equal(b.vec6[:, k], bk.vec6[:, 0]) and b.state[k] == bk.state[0]
+        if averages:
+            assert r.n_sum[k] == n_sum
+            assert np.array_equal(r.average[k], avg) and np.array_equal(r.sigma[k], sig)
+    assert 0 < n_lost < v.shape[1]
