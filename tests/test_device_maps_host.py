@@ -212,3 +212,22 @@ def test_no_read_outside_the_tables_under_asan(tmp_path):
     r = subprocess.run([sys.executable, "-c", _ASAN_CHILD.format(root=str(ROOT), so=str(so))], env=env,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and "ASAN-CLEAN" in r.stdout, (r.returncode, r.stderr[-3000:])
+
+
+def test_golden_rows_on_the_host_build(so):
+    """Every tracking_method_test row the library supports, through the
+    kernel's element maps built for the host: within the row's tolerance of
+    the reference's printed value and bit for bit equal to the correctly
+    rounded oracle (the GPU golden test, tests/test_gpu_golden.py, asks the
+    same of the GPU)."""
+    from test_oracle_golden import ELEMENTS, GOLD, START, check_row, make_element
+
+    for name in sorted(ELEMENTS):
+        lat = make_element(name)
+        hm = HostMaps(lat, so)
+        v0 = np.array(START, dtype=np.float64).reshape(6, 1)
+        b = hm.track(hm.make_bunch(v0.copy()), n_turns=1)
+        assert b.state[0] == L.ALIVE, name
+        check_row(name, b.vec6[:, 0], GOLD["tracking_method"][name])
+        ov, ob, ost, _, _ = oracle_track_elements(lat, v0.copy(), 0, 1, 1, variant="cr")
+        assert np.array_equal(b.vec6, ov) and np.array_equal(b.beta, ob), name
