@@ -13,8 +13,13 @@
   module unchanged.  ``es23.15`` keeps 16 significant digits, so an ASCII
   round trip moves coordinates by up to ~5e-16 relative.
 * The legacy ``!ASCII::3`` format (``write_ascii3_beam`` /
-  ``read_ascii3_beam``), and ``read_beam``, which tells the two apart as
-  ``read_beam_file`` does.
+  ``read_ascii3_beam``), its binary twin ``!BIN::3`` (``write_bin3_beam`` /
+  ``read_bin3_beam``: gfortran unformatted sequential records, as
+  ``read_beam_file`` reads them, beam_file_io.f90:483-495, 652-667), and
+  ``read_beam``, which tells the formats apart as ``read_beam_file`` does.
+  Per-particle charges are returned as stored, with the bunch's charge_tot;
+  ``BeamBunch.normalized_charge`` applies read_beam_file's rescaling
+  (:685-693).
 * Checkpoints (``save_checkpoint`` / ``load_checkpoint``): the exact FP64 /
   int32 arrays and the next turn index in one ``.npz`` file, so that tracking
   resumed from a checkpoint (``turn0`` = the saved turn) is bit-identical to
@@ -23,6 +28,7 @@
 """
 from __future__ import annotations
 
+import struct
 from dataclasses import dataclass
 from typing import Dict, List, Optional
 
@@ -35,6 +41,8 @@ STATE_NAME = ["Pre_Born", "Alive", "Lost", "Lost_Neg_X", "Lost_Pos_X", "Lost_Neg
               "Lost_Z"]
 # bmad_struct.f90:398-399
 LOCATION_NAME = ["GARBAGE!", "Upstream_End", "Downstream_End", "Inside"]
+# integer species codes (sim_utils/interfaces/particle_species_mod.f90:64-68)
+SPECIES_ID = {"proton": 2, "positron": 1, "electron": -1, "antiproton": -2}
 # species names (physical_constants / particle_species_mod), the ones this tracker handles
 SPECIES_MASS = {"electron": 0.51099895069e6, "positron": 0.51099895069e6, "proton": 938.27208816e6,
                 "antiproton": 938.27208816e6}
@@ -70,6 +78,21 @@ class BeamBunch:
         return cls(np.array(b.vec6, dtype=np.float64), np.array(b.state, np.int32), np.full(n, p0c),
                    np.full(n, s), np.full(n, t), np.full(n, charge), np.zeros((3, n)),
                    np.array(b.ix_ele_lost, np.int32), np.array(b.beta), species)
+
+    def normalized_charge(self) -> np.ndarray:
+        """Per-particle charges as read_beam_file leaves them
+        (beam_file_io.f90:685-693): scaled so that they sum to charge_tot,
+        or charge_tot / n each when the file gives none."""
+        q = np.asarray(self.charge, dtype=np.float64)
+        tot = self.charge_tot if self.charge_tot is not None else 0.0
+        s = 0.0
+        for v in q:  # Fortran sum order
+            s = s + v
+        if tot == 0:
+            return q.copy()
+        if s == 0:
+            return np.full(q.shape, tot / self.n)
+        return q * tot / s
 
     def to_bunch(self) -> Bunch:
         """Tracker arrays; beta from the file or, as the reader's
@@ -369,19 +392,103 @@ def read_ascii3_beam(path: str, p0c: float = 0.0) -> List[BeamBunch]:
     return out
 
 
+_BIN3_BUNCH = struct.Struct("<idddi")  # species, charge_tot, z_center, t_center, n_particle_lines
+_BIN3_PART = struct.Struct("<6ddi3dii")  # vec, charge, state, spin, ix_ele, location
+
+
+def _fortran_record(payload: bytes) -> bytes:
+    n = struct.pack("<i", len(payload))
+    return n + payload + n
+
+
+def write_bin3_beam(path: str, bunches: List[BeamBunch]) -> None:
+    """The ``!BIN::3`` layout read_beam_file reads (beam_file_io.f90:483-495,
+    652-667): gfortran unformatted sequential records, each framed by its
+    4-byte length -- the tag, (ix_ele, n_bunch, n_particle), then per bunch
+    (species, charge_tot, z_center, t_center, n) and one record per particle
+    (vec, charge, state, spin, ix_ele, location)."""
+    first = bunches[0] if bunches else None
+    ix_ele = int(first.ix_ele[0]) if first is not None and first.n else 0
+    with open(path, "wb") as f:
+        f.write(_fortran_record(b"!BIN::3"))
+        f.write(_fortran_record(struct.pack("<iii", ix_ele, len(bunches), first.n if first else 0)))
+        for b in bunches:
+            loc = LOCATION_NAME.index(b.location) if b.location in LOCATION_NAME else 2
+            charge_tot = b.charge_tot if b.charge_tot is not None else float(np.sum(b.charge))
+            f.write(_fortran_record(_BIN3_BUNCH.pack(SPECIES_ID[b.species.lower()], charge_tot, 0.0, 0.0, b.n)))
+            for j in range(b.n):
+                f.write(_fortran_record(_BIN3_PART.pack(*b.vec6[:, j], b.charge[j], int(b.state[j]), *b.spin[:, j],
+                                                        int(b.ix_ele[j]), loc)))
+
+
+def read_bin3_beam(path: str, p0c: float = 0.0) -> List[BeamBunch]:
+    """A ``!BIN::3`` beam file (see write_bin3_beam); p0c is not stored in the
+    format and is taken from the caller."""
+    data = open(path, "rb").read()
+    pos = 0
+
+    def record(what):
+        nonlocal pos
+        if pos + 4 > len(data):
+            raise ValueError(f"beam file ends before the {what}")
+        (n,) = struct.unpack_from("<i", data, pos)
+        if n < 0 or pos + 8 + n > len(data) or struct.unpack_from("<i", data, pos + 4 + n)[0] != n:
+            raise ValueError(f"bad record framing at the {what}")
+        out = data[pos + 4:pos + 4 + n]
+        pos += 8 + n
+        return out
+
+    if record("tag")[:7] != b"!BIN::3":
+        raise ValueError("not a !BIN::3 beam file")
+    ix_ele, n_bunch, n_particle = struct.unpack_from("<iii", record("header"))
+    id_to_name = {v: k for k, v in SPECIES_ID.items()}
+    out = []
+    for _ in range(n_bunch):
+        species, charge_tot, _z, _t, n_lines = _BIN3_BUNCH.unpack_from(record("bunch parameters"))
+        if species not in id_to_name:
+            raise ValueError(f"species code {species} is not handled")
+        vec = np.zeros((6, n_particle))
+        charge = np.zeros(n_particle)
+        state = np.ones(n_particle, np.int32)
+        spin = np.zeros((3, n_particle))
+        ixe = np.full(n_particle, ix_ele, np.int32)
+        loc = 2
+        j = 0
+        for j in range(1, n_lines + 1):
+            v = _BIN3_PART.unpack_from(record("particle coordinates"))
+            vec[:, j - 1] = v[0:6]
+            charge[j - 1] = v[6]
+            state[j - 1] = v[7]
+            spin[:, j - 1] = v[8:11]
+            loc = v[12]  # the particle's ix_ele is read into a scratch variable (:658)
+            if j == n_particle:
+                break
+        if j < n_particle:
+            raise ValueError(f"bunch has {j} particle records for n_particle = {n_particle}")
+        out.append(BeamBunch(vec, state, np.full(n_particle, p0c), np.zeros(n_particle), np.zeros(n_particle),
+                             charge, spin, ixe, None, id_to_name[species], LOCATION_NAME[loc],
+                             charge_tot=charge_tot))
+    return out
+
+
 def read_beam(path: str, p0c: float = 0.0) -> List[BeamBunch]:
-    """A beam file in either ASCII format, told apart as read_beam_file does
-    (beam_file_io.f90:455-476): '!ASCII::3' (or a first line that is not a
-    '#' header) is the legacy format, '#' starts the current one; binary
-    files are refused.  p0c is used by the legacy format only."""
+    """A beam file in any of the formats, told apart as read_beam_file does
+    (beam_file_io.f90:455-476) from its first 80 characters: '!BIN::3' is
+    the binary legacy format ('!BINARY' / '!BIN::2', older still, are
+    refused), '!ASCII::3' (or a first non-blank line that is not a '#'
+    header) the ASCII legacy format, '#' starts the current one.  p0c is
+    used by the legacy formats only."""
+    head = open(path, "rb").read(80)
+    if b"!BINARY" in head or b"!BIN::2" in head:
+        raise ValueError("old style binary beam files are not supported")
+    if b"!BIN::3" in head:
+        return read_bin3_beam(path, p0c)
     with open(path) as f:
         first = ""
         for ln in f:
             if ln.strip():
                 first = ln
                 break
-    if "!BINARY" in first or "!BIN::" in first:
-        raise ValueError("binary beam files are not supported")
     if first.startswith("#"):
         return read_ascii_beam(path)
     return read_ascii3_beam(path, p0c)

@@ -141,6 +141,71 @@ def test_read_beam_tells_the_formats_apart(tmp_path):
     B.write_ascii_beam(str(f), [B.BeamBunch.from_bunch(bunch, 1e9)])
     assert B.read_beam(str(f))[0].n == 3
     g = tmp_path / "bin.dat"
-    g.write_text("!BIN::3\n")
-    with pytest.raises(ValueError, match="binary"):
+    g.write_text("!BIN::3\n")  # tagged binary, but not framed as records
+    with pytest.raises(ValueError, match="framing|ends"):
         B.read_beam(str(g))
+
+
+def _bin3_bunch(n=30, seed=6, species="positron"):
+    rng = np.random.default_rng(seed)
+    state = np.ones(n, np.int32)
+    state[::5] = B.STATE_NAME.index("Lost_Neg_X")
+    return B.BeamBunch(rng.standard_normal((6, n)) * 1e-3, state, np.full(n, 5e9), np.zeros(n), np.zeros(n),
+                       rng.uniform(1e-16, 2e-16, n), rng.standard_normal((3, n)), np.full(n, 12, np.int32), None,
+                       species, charge_tot=3e-14)
+
+
+def test_bin3_round_trip_is_exact_and_detected(tmp_path):
+    a, b = _bin3_bunch(), _bin3_bunch(seed=7, species="electron")
+    f = tmp_path / "beam.bin"
+    B.write_bin3_beam(str(f), [a, b])
+    back = B.read_beam(str(f), p0c=5e9)
+    assert [r.species for r in back] == ["positron", "electron"]
+    for r, w in zip(back, (a, b)):
+        assert np.array_equal(r.vec6, w.vec6) and np.array_equal(r.spin, w.spin)
+        assert np.array_equal(r.charge, w.charge) and np.array_equal(r.state, w.state)
+        assert r.charge_tot == 3e-14 and r.location == "Downstream_End" and np.all(r.ix_ele == 12)
+
+
+def test_bin3_record_layout(tmp_path):
+    """gfortran unformatted sequential records, each framed by its 4-byte
+    length: the 7-byte tag, 3 integers, per bunch an integer species code,
+    three reals and an integer, per particle 6 + 1 reals, an integer, 3
+    reals and two integers (beam_file_io.f90:483-495, 652-667)."""
+    import struct
+
+    f = tmp_path / "beam.bin"
+    B.write_bin3_beam(str(f), [_bin3_bunch(n=2)])
+    data = f.read_bytes()
+    sizes, pos = [], 0
+    while pos < len(data):
+        (n,) = struct.unpack_from("<i", data, pos)
+        assert struct.unpack_from("<i", data, pos + 4 + n)[0] == n
+        sizes.append(n)
+        pos += 8 + n
+    assert sizes == [7, 12, 32, 92, 92]
+    assert data[4:11] == b"!BIN::3"
+    assert struct.unpack_from("<iii", data, 19) == (12, 1, 2)
+    assert struct.unpack_from("<i", data, 39)[0] == 1  # positron$ = +1
+
+
+def test_bin3_errors_and_old_binary(tmp_path):
+    f = tmp_path / "beam.bin"
+    B.write_bin3_beam(str(f), [_bin3_bunch(n=4)])
+    data = f.read_bytes()
+    (tmp_path / "cut.bin").write_bytes(data[:-10])
+    with pytest.raises(ValueError, match="framing|ends"):
+        B.read_beam(str(tmp_path / "cut.bin"))
+    (tmp_path / "old.bin").write_bytes(b"\x07\x00\x00\x00!BIN::2\x07\x00\x00\x00")
+    with pytest.raises(ValueError, match="old style binary"):
+        B.read_beam(str(tmp_path / "old.bin"))
+
+
+def test_normalized_charge_follows_read_beam_file():
+    b = _bin3_bunch(n=4)
+    q = b.normalized_charge()
+    assert np.isclose(q.sum(), 3e-14, rtol=1e-15) and np.allclose(q / b.charge, q[0] / b.charge[0])
+    b.charge[:] = 0
+    assert np.all(b.normalized_charge() == 3e-14 / 4)
+    b.charge_tot = 0.0
+    assert np.all(b.normalized_charge() == 0)
