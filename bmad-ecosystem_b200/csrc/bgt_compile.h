@@ -261,6 +261,33 @@ static void bend_mis_block(const bgt_element& e, double* bm) {
   }
 }
 
+// The BMA block: offset_particle's set transform at s_pos = 0 and s_pos = L
+// without the drift (offset_particle.f90:208-228), up to the arc shift that
+// depends on the particle.
+static void bend_ap_block(const bgt_element& e, double* bma) {
+  const double g = e.g, rt = e.ref_tilt, L = e.l, L_half = 0.5 * L;
+  const double zero[3] = {0.0, 0.0, 0.0};
+  double L_mis[3], ws[3][3], wt[3][3], wm[3][3];
+  bend_L_S(e, L_mis, ws);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) wt[i][j] = ws[j][i];
+  bma[BMA_G] = g;
+  for (int end = 0; end < 2; end++) {
+    const double ds_center = L_half - (end == 0 ? 0.0 : L);
+    BendChain c(bma + (end == 0 ? BMA_OPS_IN : BMA_OPS_OUT));
+    c.shift(g, 1 * ds_center, true, rt);
+    c.op(2, wt, L_mis);
+    if (rt != 0) {
+      c.shift(g, -L_half, true, rt);
+      w_tilt_h(-rt, wm);
+      c.op(3, wm, zero);
+      c.shift(g, L_half, false, 0.0);
+    }
+    bma[end == 0 ? BMA_NIN : BMA_NOUT] = c.n;
+    bma[end == 0 ? BMA_DSC_IN : BMA_DSC_OUT] = ds_center;
+  }
+}
+
 struct Builder {
   std::vector<double>& out;
   size_t start;
@@ -406,11 +433,21 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     }
   }
   if (ap_any) {
-    if (e.offset_moves_aperture && (flags & F_MISALIGN) && (offset || tilt != 0)) {
-      if (kind == K_BEND) {
-        err = ename(e) + ": offset_moves_aperture on a bend is not supported";
-        return BGT_EUNSUPPORTED;
+    if (kind == K_BEND) {
+      // offset_particle(set, s_pos, no tilt) of a bend (offset_particle.f90:
+      // 180-258): the bend geometry when misaligned with g, ref_tilt or roll
+      // (BMA block), the straight geometry when misaligned otherwise, and a
+      // bare ref_tilt rotation when not misaligned
+      const bool misaligned = offset || e.roll != 0;
+      if (e.offset_moves_aperture && (misaligned || e.ref_tilt != 0)) {
+        if (!(flags & F_MISALIGN)) {
+          err = ename(e) + ": offset_moves_aperture on a bend with ref_tilt needs has_misalign set";
+          return BGT_EUNSUPPORTED;
+        }
+        flags |= F_AP_OFFSET;
+        if (!misaligned) flags |= F_AP_TILT;
       }
+    } else if (e.offset_moves_aperture && (flags & F_MISALIGN) && (offset || tilt != 0)) {
       flags |= F_AP_OFFSET;
       if (key == BGT_ECOLLIMATOR || key == BGT_RCOLLIMATOR) flags |= F_AP_TILT;
     }
@@ -465,6 +502,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
     double s_lab = m[MIS_R3UNSET] + m[MIS_ZADD];
     m[MIS_DS_UNSET] = (1 + 1) * L_half - s_lab;
     if (flags & F_BEND_MIS) bend_mis_block(e, B.ptr_after_push(BM_N));
+    if ((flags & F_BEND_MIS) && (flags & F_AP_OFFSET)) bend_ap_block(e, B.ptr_after_push(BMA_N));
   }
   if (flags & (F_AP_ENTRANCE | F_AP_EXIT)) {
     double* a = B.ptr_after_push(AP_N);

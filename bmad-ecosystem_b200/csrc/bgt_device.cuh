@@ -90,8 +90,84 @@ static __constant__ double c_cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
 // multipole_mod.f90:262-266).
 static __constant__ double c_cm0[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
 
+// 3x3 matrix times vector, sums from zero in k order (as the oracle's and
+// gfortran's matmul)
+__device__ __forceinline__ void mv3_0(const double* S, double r0, double r1, double r2, double& o0, double& o1,
+                                      double& o2) {
+  o0 = ((0.0 + S[0] * r0) + S[1] * r1) + S[2] * r2;
+  o1 = ((0.0 + S[3] * r0) + S[4] * r1) + S[5] * r2;
+  o2 = ((0.0 + S[6] * r0) + S[7] * r1) + S[8] * r2;
+}
+
+// A position (r0, r1, r2) through a host-recorded chain of affine steps of a
+// misaligned bend's geometry (bend_shift, misalignment and tilt frames; the
+// op layout of the BM block in bgt_table.h).
+__device__ __forceinline__ void bend_chain_position(const double* ops, int n, double& r0, double& r1, double& r2) {
+  for (int k = 0; k < n; k++) {
+    const double* o = ops + k * BM_OP_N;
+    const int code = (int)o[0];
+    const double* S = o + 1;
+    const double* L = o + 10;
+    if (code == 0) {
+      r2 = r2 - L[2];
+    } else if (code == 4) {
+      r2 = r2 + L[2];
+    } else {
+      double a0 = r0, a1 = r1, a2 = r2;
+      if (code == 2) {
+        a0 = r0 - L[0];
+        a1 = r1 - L[1];
+        a2 = r2 - L[2];
+      }
+      mv3_0(S, a0, a1, a2, r0, r1, r2);
+      if (code == 1) {
+        r0 = r0 + L[0];
+        r1 = r1 + L[1];
+        r2 = r2 + L[2];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Apertures
+
+// The element frame of a misaligned bend at an end for the aperture check:
+// offset_particle(set, s_pos = 0 or L, no drift, no tilt),
+// offset_particle.f90:208-228 and 246-258 (only x and y are needed).  The
+// chain up to the arc shift is element-constant (BMA block); the shift by
+// ds = rho atan2(r3 g, 1 + r1 g) turns by a particle-dependent angle, so its
+// rotation (bend_shift.f90:19-61 without ref_tilt) runs here.  Out of line,
+// like the exact bend edge, so that it adds no register pressure to the
+// element loop.
+struct XY {
+  double x, y;
+};
+BGT_DEV_NOINLINE XY bend_aperture_frame(Part p, const double* bma, bool at_exit) {
+  double r0 = p.x, r1 = p.y, r2 = 0.0;
+  bend_chain_position(bma + (at_exit ? BMA_OPS_OUT : BMA_OPS_IN), (int)bma[at_exit ? BMA_NOUT : BMA_NIN], r0, r1,
+                      r2);
+  const double g = bma[BMA_G];
+  const double ds = (g == 0) ? -1 * bma[at_exit ? BMA_DSC_OUT : BMA_DSC_IN]
+                             : (1 / g) * cr::atan2(r2 * g, 1.0 + r0 * g);
+  const double angle = ds * g;
+  if (angle != 0) {
+    const double ca = cr::cos(angle), sa = cr::sin(angle);
+    // rotate_mat(unit, y, angle): each column of the unit matrix as rotate_vec
+    const double S[9] = {sa * 0.0 + ca * 1.0, sa * 0.0 + ca * 0.0, sa * 1.0 + ca * 0.0,
+                         0.0, 1.0, 0.0,
+                         ca * 0.0 - sa * 1.0, ca * 0.0 - sa * 0.0, ca * 1.0 - sa * 0.0};
+    const double sh = cr::sin(angle / 2);
+    double o0, o1, o2;
+    mv3_0(S, r0, r1, r2, o0, o1, o2);
+    r0 = o0 + -(2 * (sh * sh)) / g;
+    r1 = o1 + 0.0 / g;
+  }
+  const double rel_p = 1 + p.pz;
+  const double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;
+  if (pz > 0) return {r0, r1};  // with pz <= 0 offset_particle only marks the particle
+  return {p.x, p.y};
+}
 
 // bmad/low_level/orbit_too_large.f90:26-120
 __device__ __forceinline__ bool orbit_too_large(Part& p, const Glob& G) {
@@ -137,6 +213,12 @@ __device__ __forceinline__ void aperture_frame(const Part& p, const double* mis,
   xa = p.x;
   ya = p.y;
   if (!(flags & F_AP_OFFSET)) return;
+  if (flags & F_BEND_MIS) {
+    const XY f = bend_aperture_frame(p, mis + MIS_N + BM_N, at_exit);
+    xa = f.x;
+    ya = f.y;
+    return;
+  }
   if (flags & F_OFFSET) {
     if (flags & F_PITCH) {
       const double rel_p = 1 + p.pz;

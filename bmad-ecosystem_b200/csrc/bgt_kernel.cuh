@@ -52,7 +52,10 @@ __device__ __forceinline__ Rec decode(const double* r) {
   if (fl & F_MISALIGN) {
     R.mis = q;
     q += MIS_N;
-    if (RARE && (fl & F_BEND_MIS)) q += BM_N;  // the bend geometry follows the block
+    if (RARE && (fl & F_BEND_MIS)) {
+      q += BM_N;  // the bend geometry follows the block
+      if (fl & F_AP_OFFSET) q += BMA_N;  // and its aperture frames
+    }
   }
   if (fl & (F_AP_ENTRANCE | F_AP_EXIT)) {
     R.ap = q;
@@ -427,15 +430,6 @@ __device__ __forceinline__ void bend_elec_kicks(Part& p, const double* ae, const
   p.z = z0 * p.beta / beta0;
 }
 
-// 3x3 matrix times vector, sums from zero in k order (as the oracle's and
-// gfortran's matmul)
-__device__ __forceinline__ void mv3_0(const double* S, double r0, double r1, double r2, double& o0, double& o1,
-                                      double& o2) {
-  o0 = ((0.0 + S[0] * r0) + S[1] * r1) + S[2] * r2;
-  o1 = ((0.0 + S[3] * r0) + S[4] * r1) + S[5] * r2;
-  o2 = ((0.0 + S[6] * r0) + S[7] * r1) + S[8] * r2;
-}
-
 // offset_particle for a misaligned bend (offset_particle.f90:208-235 set,
 // :393-425 unset, drift to the edge): (x, y, 0) through the BM block's
 // affine steps, the momentum through their product W, then the drift to the
@@ -446,30 +440,7 @@ __device__ __forceinline__ void bend_offset(Part& p, const double* bm, bool set,
   const double* ops = bm + (set ? BM_OPS_SET : BM_OPS_UNSET);
   const double* W = bm + (set ? BM_WSET : BM_WUNSET);
   double r0 = p.x, r1 = p.y, r2 = 0.0;
-  for (int k = 0; k < n; k++) {
-    const double* o = ops + k * BM_OP_N;
-    const int code = (int)o[0];
-    const double* S = o + 1;
-    const double* L = o + 10;
-    if (code == 0) {
-      r2 = r2 - L[2];
-    } else if (code == 4) {
-      r2 = r2 + L[2];
-    } else {
-      double a0 = r0, a1 = r1, a2 = r2;
-      if (code == 2) {
-        a0 = r0 - L[0];
-        a1 = r1 - L[1];
-        a2 = r2 - L[2];
-      }
-      mv3_0(S, a0, a1, a2, r0, r1, r2);
-      if (code == 1) {
-        r0 = r0 + L[0];
-        r1 = r1 + L[1];
-        r2 = r2 + L[2];
-      }
-    }
-  }
+  bend_chain_position(ops, n, r0, r1, r2);
   const double s_pos = r2;
   const double rel_p = 1 + p.pz;
   const double pz = rel_p * rel_p - p.px * p.px - p.py * p.py;

@@ -135,6 +135,13 @@ constexpr int BM_WSET = 2, BM_WUNSET = 11;  // 9 doubles each, row-major
 constexpr int BM_OP_N = 13, BM_MAX_OPS = 7;
 constexpr int BM_OPS_SET = 20, BM_OPS_UNSET = BM_OPS_SET + BM_MAX_OPS * BM_OP_N;
 constexpr int BM_N = BM_OPS_UNSET + BM_MAX_OPS * BM_OP_N;
+// Bend aperture-frame block (F_BEND_MIS with F_AP_OFFSET), after the BM
+// block: offset_particle(set, s_pos = 0 or L, no drift, no tilt) as
+// check_aperture_limit.f90:159-175 calls it.  Per end the affine steps up to
+// the particle-dependent arc shift (op layout as above) and ds_center; g.
+constexpr int BMA_NIN = 0, BMA_NOUT = 1, BMA_G = 2, BMA_DSC_IN = 3, BMA_DSC_OUT = 4;
+constexpr int BMA_OPS_IN = 5, BMA_OPS_OUT = BMA_OPS_IN + BM_MAX_OPS * BM_OP_N;
+constexpr int BMA_N = BMA_OPS_OUT + BM_MAX_OPS * BM_OP_N;
 
 constexpr int AP_X1 = 0, AP_X2 = 1, AP_Y1 = 2, AP_Y2 = 3;  // x1_lim = -x1_limit, ...
 constexpr int AP_XW = 4, AP_XC = 5, AP_YW = 6, AP_YC = 7;  // elliptical width2/center

@@ -988,6 +988,36 @@ static void bend_shift(bgo_pos* p, double g, double delta_s, int has_tilt, doubl
   matmul33(S, p->w, p->w);
 }
 
+/* bend_shift for a particle-dependent arc length (the s_pos form of the bend
+ * geometry): the same operations, with the rotation by the particle's angle
+ * taken through the particle transcendentals (P_SIN / P_COS); ref_tilt
+ * rotations, element constants, through the C library. */
+static void bend_shift_particle(bgo_pos* p, double g, double delta_s, int has_tilt, double ref_tilt) {
+  double angle = delta_s * g;
+  if (angle == 0) {
+    p->r[2] = p->r[2] - delta_s;
+    return;
+  }
+  double tlt = has_tilt ? ref_tilt : 0.0;
+  double S[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  if (tlt != 0) rotate_mat(S, AX_Z, -ref_tilt);
+  double ca = P_COS(angle), sa = P_SIN(angle);
+  for (int j = 0; j < 3; j++) { /* rotate_mat(S, AX_Y, angle), each column as rotate_vec */
+    double a = sa * S[2][j] + ca * S[0][j];
+    double b = ca * S[2][j] - sa * S[0][j];
+    S[0][j] = a;
+    S[2][j] = b;
+  }
+  if (tlt != 0) rotate_mat(S, AX_Z, ref_tilt);
+  double sh = P_SIN(angle / 2);
+  double L[3] = {-(2 * (sh * sh)) / g, 0.0 / g, -sa / g};
+  if (has_tilt) rotate_vec(L, AX_Z, ref_tilt);
+  double r[3];
+  matvec3(S, p->r, r);
+  for (int i = 0; i < 3; i++) p->r[i] = r[i] + L[i];
+  matmul33(S, p->w, p->w);
+}
+
 /* ele_misalignment_L_S_calc, bmad/geometry/ele_misalignment_L_S_calc.f90:
  * 16-50, sbend branch (angle = g L, rho = 1/g as the bookkeeper sets them) */
 static void bend_misalignment_L_S(const bgo_ele* ele, double L_mis[3], double S[3][3]) {
@@ -1037,7 +1067,7 @@ static void bend_offset_position(const bgo_ele* ele, int set, int drift_to, doub
       pos->r[2] = pos->r[2] + (1 - 1 * 1) * L_half;
     } else {
       double ds = (g == 0) ? -1 * ds_center : (1 / g) * P_ATAN2(pos->r[2] * g, 1.0 + pos->r[0] * g);
-      bend_shift(pos, g, ds, 0, 0.0);
+      bend_shift_particle(pos, g, ds, 0, 0.0);
       pos->r[2] = pos->r[2] + L_half + ds;
     }
   } else {
@@ -1056,7 +1086,7 @@ static void bend_offset_position(const bgo_ele* ele, int set, int drift_to, doub
       pos->r[2] = pos->r[2] + (1 + 1 * 1) * L_half;
     } else {
       double ds = (g == 0) ? -ds_center : (1 / g) * P_ATAN2(pos->r[2] * g, 1.0 + pos->r[0] * g);
-      bend_shift(pos, g, ds, 1, ref_tilt);
+      bend_shift_particle(pos, g, ds, 1, ref_tilt);
       pos->r[2] = pos->r[2] + L_half + ds;
     }
   }

@@ -140,6 +140,16 @@ def rare_zoo_lattice() -> L.Lattice:
                                                 "z_aperture_width2": 0.013}))
     E.append(L.Element("rcollimator", "RCMOM", {"l": 0.1, "pz_aperture_width2": 0.011, "pz_aperture_center": 5e-4,
                                                 "py_aperture_width2": 7e-4}))
+    # apertures that move with a bend (offset_moves_aperture): the curved
+    # misaligned geometry, a bare ref_tilt and the straight (g = 0) geometry
+    ap = {"x1_limit": 0.012, "x2_limit": 0.013, "y1_limit": 0.006, "y2_limit": 0.0065}
+    E.append(L.Element("sbend", "BMISAP", {"l": 0.9, "g": 0.015, "e1": 0.02, "x_offset": 4e-4, "y_offset": -3e-4,
+                                           "z_offset": 2e-3, "x_pitch": 2e-4, "y_pitch": 1e-4, "ref_tilt": 0.07,
+                                           **ap}, offset_moves_aperture=True, aperture_at="both_ends"))
+    E.append(L.Element("sbend", "BTILTAP", {"l": 0.6, "g": 0.01, "ref_tilt": 0.3, **ap}, offset_moves_aperture=True,
+                       aperture_type="elliptical", aperture_at="both_ends"))
+    E.append(L.Element("sbend", "BSTRAP", {"l": 0.5, "k1": 0.05, "x_offset": 5e-4, "y_pitch": 2e-4, **ap},
+                       offset_moves_aperture=True, aperture_at="both_ends"))
     lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "rare_zoo")
     return lat.finalize()
 

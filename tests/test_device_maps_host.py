@@ -231,3 +231,30 @@ def test_golden_rows_on_the_host_build(so):
         check_row(name, b.vec6[:, 0], GOLD["tracking_method"][name])
         ov, ob, ost, _, _ = oracle_track_elements(lat, v0.copy(), 0, 1, 1, variant="cr")
         assert np.array_equal(b.vec6, ov) and np.array_equal(b.beta, ob), name
+
+
+def test_apertures_that_move_with_bends(so, oracle_lib):
+    """offset_moves_aperture on bends with tight limits, so that the frame
+    decides hundreds of losses: the curved misaligned geometry at both ends
+    (the arc shift by a particle-dependent angle), a bare ref_tilt, the
+    straight geometry, elliptical and rectangular."""
+    ap = {"x1_limit": 0.004, "x2_limit": 0.0045, "y1_limit": 0.002, "y2_limit": 0.0025}
+    E = [L.Element("sbend", "BMISAP", {"l": 0.9, "g": 0.015, "e1": 0.02, "x_offset": 4e-4, "y_offset": -3e-4,
+                                       "z_offset": 2e-3, "x_pitch": 2e-4, "y_pitch": 1e-4, "ref_tilt": 0.07, **ap},
+                   offset_moves_aperture=True, aperture_at="both_ends"),
+         L.Element("sbend", "BROLLAP", {"l": 1.2, "g": -0.02, "roll": 3e-3, "x_offset": 2e-4, **ap},
+                   offset_moves_aperture=True, aperture_type="elliptical", aperture_at="exit_end"),
+         L.Element("sbend", "BTILTAP", {"l": 0.6, "g": 0.01, "ref_tilt": 0.3, **ap}, offset_moves_aperture=True,
+                   aperture_type="elliptical", aperture_at="both_ends"),
+         L.Element("sbend", "BSTRAP", {"l": 0.5, "k1": 0.05, "x_offset": 5e-4, "y_pitch": 2e-4, **ap},
+                   offset_moves_aperture=True, aperture_at="both_ends")]
+    lat = L.Lattice(E, L.Species("electron", L.M_ELECTRON, -1), rings.p0c(), rings.E_TOT, "moving_apertures")
+    lat.finalize()
+    hm = HostMaps(lat, so)
+    assert hm.needs_rare
+    v0 = random_particles(2000, seed=37)
+    for pos, ele in enumerate(lat.elements):
+        b = hm.track(hm.make_bunch(v0.copy()), pos, pos + 1, turns=False)
+        ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
+        assert (ost != L.ALIVE).sum() > 200, ele.name
+        assert_bitwise(b, ov, ob, ost, oie, what=ele.name)

@@ -71,8 +71,6 @@ def _line(key, values, **kw):
 
 @pytest.mark.parametrize("key,values,kw,msg", [
     ("sbend", {"l": 1.0, "g": 0.01}, {"exact_multipoles": 1}, "exact_multipoles"),
-    ("sbend", {"l": 1.0, "g": 0.01, "x_offset": 1e-4, "x1_limit": 0.02, "x2_limit": 0.02, "y1_limit": 0.01,
-               "y2_limit": 0.01}, {"offset_moves_aperture": True}, "offset_moves_aperture"),
     ("drift", {"l": 1.0}, {"b_pole_elec": {1: 1e5}}, "electric multipoles"),
 ])
 def test_unsupported_elements_are_rejected_and_named(key, values, kw, msg, capfd):
