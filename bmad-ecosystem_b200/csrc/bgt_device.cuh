@@ -46,9 +46,10 @@ struct DriftMemo {
   double a;
 };
 
-// Out-of-line device functions (a plain static function in a host build).
+// Out-of-line device functions (a plain static function in a host build);
+// internal linkage, since every compilation unit of kernels has its own copy.
 #ifdef __CUDACC__
-#define BGT_DEV_NOINLINE __device__ __noinline__
+#define BGT_DEV_NOINLINE static __device__ __noinline__
 #else
 #define BGT_DEV_NOINLINE static __attribute__((noinline))
 #endif
