@@ -19,7 +19,8 @@ from bgt import rings
 from bgt.track import Bunch, Tracker
 
 from helpers import (RTOL_1000_TURNS, RTOL_LIBM_1000_TURNS, RTOL_LIBM_ONE_TURN, RTOL_ONE_TURN,
-                     oracle_track_elements, random_particles, rare_zoo_lattice, rel_err, zoo_lattice)
+                     oracle_track_elements, random_particles, rare_zoo_lattice, rel_err, rtol_vs_glibc_one_element,
+                     zoo_lattice)
 
 pytestmark = pytest.mark.gpu
 
@@ -90,7 +91,7 @@ def test_rare_zoo_each_element_bitwise(rare_zoo):
         assert_bitwise(b, ov, ob, ost, oie, what=ele.name)
         ovg, _, ostg, _, _ = oracle_track_elements(lat, v0, pos, pos + 1)
         assert np.array_equal(b.state, ostg), f"{ele.name}: state vs glibc oracle"
-        assert np.all(rel_err(b.vec6, ovg, ostg == L.ALIVE) <= RTOL_ONE_TURN), ele.name
+        assert np.all(rel_err(b.vec6, ovg, ostg == L.ALIVE) <= rtol_vs_glibc_one_element(ele)), ele.name
 
 
 def test_rare_zoo_turns_with_losses(rare_zoo):
