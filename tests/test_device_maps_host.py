@@ -258,3 +258,26 @@ def test_apertures_that_move_with_bends(so, oracle_lib):
         ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
         assert (ost != L.ALIVE).sum() > 200, ele.name
         assert_bitwise(b, ov, ob, ost, oie, what=ele.name)
+
+
+def test_elements_switched_off(so, oracle_lib):
+    """Every element of both zoos with is_on = F (track1_bmad.f90:51-60: an
+    off bend keeps its edges with g_tot = 0, everything else but thin
+    multipoles becomes a drift), through the host build against the oracle."""
+    import copy
+
+    v0 = random_particles(512, seed=38)
+    for make in (zoo_lattice, rare_zoo_lattice):
+        base = make()
+        E = []
+        for e in base.elements:
+            c = copy.deepcopy(e)
+            c.is_on = False
+            E.append(c)
+        lat = L.Lattice(E, base.species, base.p0c, base.e_tot, base.name + "_off")
+        lat.finalize()
+        hm = HostMaps(lat, so)
+        for pos, ele in enumerate(lat.elements):
+            b = hm.track(hm.make_bunch(v0.copy()), pos, pos + 1, turns=False)
+            ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
+            assert_bitwise(b, ov, ob, ost, oie, what=ele.name + " (off)")
