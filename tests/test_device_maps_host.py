@@ -281,3 +281,29 @@ def test_elements_switched_off(so, oracle_lib):
             b = hm.track(hm.make_bunch(v0.copy()), pos, pos + 1, turns=False)
             ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
             assert_bitwise(b, ov, ob, ost, oie, what=ele.name + " (off)")
+
+
+def test_loss_branches_with_extreme_particles(so, oracle_lib):
+    """Particles far outside the beam (30x its size) and hand-made ones past
+    the momentum limits (|px| >= 1 + pz: lost_pz in drifts and bodies;
+    1 + pz < 0: orbit_too_large), through every element of both zoos, with
+    coordinates that may end as NaN compared NaN-aware.  Arguments stay in
+    the correctly rounded ranges of bgt::cr (beyond them, e.g. cosh of a
+    body phase past 2 when 1 + pz -> 0, both builds use the library and are
+    not held to each other)."""
+    v0 = random_particles(1024, seed=39, scale=30.0)
+    v0[1, :40] = np.linspace(-1.6, 1.6, 40)  # |px| past the total momentum
+    v0[5, 40:60] = np.linspace(-2.5, -1.05, 20)  # 1 + pz < 0
+    seen = set()
+    for make in (zoo_lattice, rare_zoo_lattice):
+        lat = make()
+        hm = HostMaps(lat, so)
+        for pos, ele in enumerate(lat.elements):
+            b = hm.track(hm.make_bunch(v0.copy()), pos, pos + 1, turns=False)
+            ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, pos, pos + 1, variant="cr")
+            assert np.array_equal(b.state, ost), ele.name
+            assert np.array_equal(b.ix_ele_lost, oie), ele.name
+            assert np.array_equal(b.vec6, ov, equal_nan=True), ele.name
+            assert np.array_equal(b.beta, ob, equal_nan=True), ele.name
+            seen.update(int(s) for s in np.unique(ost))
+    assert {L.ALIVE, L.LOST_NEG_X, L.LOST_POS_X, L.LOST_NEG_Y, L.LOST_POS_Y, L.LOST_PZ} <= seen
