@@ -307,3 +307,28 @@ def test_loss_branches_with_extreme_particles(so, oracle_lib):
             assert np.array_equal(b.beta, ob, equal_nan=True), ele.name
             seen.update(int(s) for s in np.unique(ost))
     assert {L.ALIVE, L.LOST_NEG_X, L.LOST_POS_X, L.LOST_NEG_Y, L.LOST_POS_Y, L.LOST_PZ} <= seen
+
+
+@pytest.mark.parametrize("make", [zoo_lattice, rare_zoo_lattice], ids=["zoo", "rare_zoo"])
+def test_each_element_alone_picks_a_kernel_that_handles_it(so, oracle_lib, make):
+    """Each element alone in a line of its own, so that the host picks the
+    kernel instance from that one record: a rare feature missing from the
+    RARE selection would run on the lean kernel, which skips it, and differ
+    from the oracle.  No zoo element needs the RARE instance; all rare-zoo
+    elements do but its drift and the misaligned straight (g = 0) bend, which
+    the lean kernel handles."""
+    base = make()
+    v0 = random_particles(256, seed=40)
+    lean = []
+    for ele in base.elements:
+        lat = L.Lattice([ele], base.species, base.p0c, base.e_tot, ele.name)
+        hm = HostMaps(lat, so)
+        if not hm.needs_rare:
+            lean.append(ele.name)
+        b = hm.track(hm.make_bunch(v0.copy()), turns=False)
+        ov, ob, ost, oie, _ = oracle_track_elements(lat, v0, 0, 1, variant="cr")
+        assert_bitwise(b, ov, ob, ost, oie, what=ele.name + " alone")
+    if make is rare_zoo_lattice:
+        assert lean == ["D", "BSTRAIGHT"]
+    else:
+        assert lean == [e.name for e in base.elements]
