@@ -83,9 +83,13 @@ def test_drift_to_edges_and_track(name, oracle_lib):
     _check(f"{name} unset", orb, _row(name, "Drift-Out"), s.value)
 
 
+@pytest.mark.parametrize("variant", ["glibc", "cr"])
 @pytest.mark.parametrize("name", ["Q1", "B0", "B1", "B2"])
-def test_at_a_given_s(name, oracle_lib):
-    lib = oracle_lib
+def test_at_a_given_s(name, variant, oracle_lib):
+    # the "cr" build takes the arc shift by the particle-dependent angle with
+    # correctly rounded transcendentals, as the device's moving bend
+    # apertures do
+    lib = oracle_lib if variant == "glibc" else O.load(variant="cr")
     ele, p0c = _ele(*ELEMENTS[name], lib)
     param = O.make_param(L.M_ELECTRON, -1)
     start = _row(name, "Static-Start")
