@@ -44,7 +44,8 @@ class BgtSpecies(C.Structure):
 
 class BgtTuning(C.Structure):
     _fields_ = [("threads_per_block", C.c_int32), ("blocks_per_sm", C.c_int32), ("turns_per_launch", C.c_int32),
-                ("compact_every", C.c_int32), ("table_mode", C.c_int32)]
+                ("compact_every", C.c_int32), ("table_mode", C.c_int32), ("wait_limit_us", C.c_int32),
+                ("test_skip_table_copy", C.c_int32)]
 
 
 class BgtError(RuntimeError):
@@ -56,7 +57,7 @@ _lib = None
 # every symbol include/bgt.h and include/bgt_mlp.h declare
 EXPORTED = [
     "bgt_create", "bgt_destroy", "bgt_last_error", "bgt_table_info", "bgt_set_tuning", "bgt_get_tuning",
-    "bgt_track_turns", "bgt_track_turns_device", "bgt_track_elements", "bgt_da_scan_grid",
+    "bgt_track_turns", "bgt_track_turns_device", "bgt_device_status", "bgt_track_elements", "bgt_da_scan_grid",
     "bgt_kernel_launch_count", "bgt_fp64_peak_tflops", "bgt_track_turns_device_noalloc",
     # include/bgt_mlp.h
     "bgt_mlp_create", "bgt_mlp_destroy", "bgt_mlp_last_error", "bgt_mlp_launch_count", "bgt_mlp_get_params",
@@ -89,16 +90,17 @@ def load() -> C.CDLL:
     lib.bgt_track_turns.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _ip, C.c_int64, C.c_int32, C.c_int32]
     lib.bgt_track_turns_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
+    lib.bgt_device_status.argtypes = [C.c_void_p, C.c_void_p]
     lib.bgt_track_elements.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, C.c_int64, C.c_int32, C.c_int32]
-    lib.bgt_da_scan_grid.argtypes = [C.c_void_p, _dp, C.c_int32, _dp, C.c_int32, C.c_int32, C.c_double, C.c_double,
+    lib.bgt_da_scan_grid.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                      C.c_int32, C.c_double, C.c_double, C.c_int32, _dp, _ip]
     lib.bgt_kernel_launch_count.argtypes = [C.c_void_p]
     lib.bgt_kernel_launch_count.restype = C.c_int64
     lib.bgt_fp64_peak_tflops.argtypes = [C.c_int32, _dp]
     lib.bgt_track_turns_device_noalloc.argtypes = [
         C.POINTER(BgtElement), C.c_int32, C.POINTER(BgtSpecies), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-        C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.POINTER(BgtTuning), C.c_int32, C.c_void_p, C.c_char_p,
-        C.c_int32]
+        C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.POINTER(BgtTuning), C.c_int32, C.c_void_p, C.c_void_p,
+        C.c_char_p, C.c_int32]
     _lib = lib
     return lib
 

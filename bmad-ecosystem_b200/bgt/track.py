@@ -96,15 +96,17 @@ class Tracker:
         h = C.c_void_p()
         rc = self.lib.bgt_create(C.byref(h), arr, n_ele, len(lats), C.byref(sp), device)
         if rc != 0:
-            raise _lib.BgtError(f"bgt_create failed ({rc}); see stderr for the element")
+            raise _lib.BgtError(f"bgt_create failed ({rc}): {self.lib.bgt_last_error(None).decode()}")
         self.h = h
         self.device = device
         if tuning:
             self.set_tuning(**tuning)
 
     # -- tuning -----------------------------------------------------------
-    def set_tuning(self, threads_per_block=0, blocks_per_sm=0, turns_per_launch=0, compact_every=0, table_mode=0):
-        t = _lib.BgtTuning(threads_per_block, blocks_per_sm, turns_per_launch, compact_every, table_mode)
+    def set_tuning(self, threads_per_block=0, blocks_per_sm=0, turns_per_launch=0, compact_every=0, table_mode=0,
+                   wait_limit_us=0, test_skip_table_copy=0):
+        t = _lib.BgtTuning(threads_per_block, blocks_per_sm, turns_per_launch, compact_every, table_mode,
+                           wait_limit_us, test_skip_table_copy)
         _check(self.lib, self.h, self.lib.bgt_set_tuning(self.h, C.byref(t)), "bgt_set_tuning")
 
     def get_tuning(self) -> dict:
@@ -184,6 +186,17 @@ class Tracker:
                                              n_turns, C.c_void_p(stream.cuda_stream))
         _check(self.lib, self.h, rc, "bgt_track_turns_device")
 
+    def device_status(self, stream=None):
+        """Wait for `stream` (default: the current stream) and raise BgtError
+        if a device-buffer call since the last check hit a table-staging
+        timeout on the device (the flag is cleared)."""
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream(torch.device("cuda", self.device))
+        rc = self.lib.bgt_device_status(self.h, C.c_void_p(stream.cuda_stream))
+        _check(self.lib, self.h, rc, "bgt_device_status")
+
     def da_scan_grid(self, ref_orbit: np.ndarray, n_angle: int, angle_min: float, angle_max: float,
                      n_radius: int, r_max: float, y_scale: float, n_turns: int, n_variants: Optional[int] = None,
                      return_survival: bool = False):
@@ -195,10 +208,8 @@ class Tracker:
         nd = ref.shape[1]
         out = np.zeros((nv, nd, n_angle), dtype=np.float64)
         surv = np.zeros((nv, nd, n_angle, n_radius), dtype=np.int32) if return_survival else None
-        deltas = np.zeros(nd)
-        rc = self.lib.bgt_da_scan_grid(self.h, _lib.ptr(ref, C.c_double), nv, _lib.ptr(deltas, C.c_double), nd,
-                                       n_angle, angle_min, angle_max, n_radius, r_max, y_scale, n_turns,
-                                       _lib.ptr(out, C.c_double),
+        rc = self.lib.bgt_da_scan_grid(self.h, _lib.ptr(ref, C.c_double), nv, nd, n_angle, angle_min, angle_max,
+                                       n_radius, r_max, y_scale, n_turns, _lib.ptr(out, C.c_double),
                                        _lib.ptr(surv, C.c_int32) if surv is not None else None)
         _check(self.lib, self.h, rc, "bgt_da_scan_grid")
         return (out, surv) if return_survival else out

@@ -21,6 +21,8 @@
 
 #ifdef __CUDACC__
 #include <cuda_runtime.h>
+
+#include <atomic>
 #endif
 #include <math.h>
 #include <stdint.h>
@@ -705,18 +707,29 @@ __device__ __forceinline__ void tma_bulk_g2s(void* dst, const void* src, uint32_
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-// Bounded wait on the mbarrier phase.  Returns false after max_iters tries.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t max_iters) {
-  for (uint32_t it = 0; it < max_iters; it++) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (done) return true;
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait on the mbarrier phase: false once limit_ns nanoseconds of
+// %globaltimer have passed without the phase completing.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > limit_ns) return false;
   }
-  return false;
+  return true;
 }
 
 // ===========================================================================
@@ -745,7 +758,10 @@ struct KArgs {
   int32_t turn0, n_turns;
   int32_t compact_every;
   int32_t* tile_counter;
-  int32_t* error_flag;
+  int32_t* error_flag;            // this call's flag: 1 = a table-staging wait ran out
+  int32_t* status;                // the handle's sticky flag (ORed with error_flag; may be null)
+  uint64_t wait_ns;               // bound of every wait on the staging mbarrier
+  int32_t skip_table_copy;        // test only: arm the mbarrier but issue no copy, so the wait runs out
   Glob G;
 };
 
@@ -875,11 +891,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
       // all threads finished reading the previous table (barrier above)
       if (tid == 0) {
         mbar_expect_tx(&bar, table_bytes);
-        tma_bulk_g2s(smem, a.tables + a.table_off_dw[variant], table_bytes, &bar);
+        if (!a.skip_table_copy) tma_bulk_g2s(smem, a.tables + a.table_off_dw[variant], table_bytes, &bar);
       }
-      const int bad = __syncthreads_or(!mbar_wait(&bar, parity, 1u << 26));
+      const int bad = __syncthreads_or(!mbar_wait(&bar, parity, a.wait_ns));
       if (bad) {
-        if (tid == 0) atomicExch(a.error_flag, 1);
+        // Give the copy in flight (if one was issued) one more bounded wait
+        // to land before the CTA's shared memory is released, then report.
+        if (tid == 0) {
+          if (!a.skip_table_copy) mbar_wait(&bar, parity, a.wait_ns);
+          atomicExch(a.error_flag, 1);
+          if (a.status) atomicOr(a.status, 1);
+        }
         return;
       }
       parity ^= 1u;
@@ -1034,14 +1056,16 @@ constexpr size_t SMEM_LIMIT = 224 * 1024;
 
 template <int BLOCK, int MINB, int TMODE, bool RARE>
 cudaError_t launch_track(const KArgs& a, int grid, size_t smem, cudaStream_t st) {
-  static bool attr_set[64] = {};
+  // the attribute is per device; setting it twice (two threads racing on
+  // the first launch) is harmless
+  static std::atomic<bool> attr_set[64];
   int dev = 0;
   cudaGetDevice(&dev);
-  if (!attr_set[dev & 63]) {
+  if (!attr_set[dev & 63].load(std::memory_order_acquire)) {
     cudaError_t e = cudaFuncSetAttribute(track_kernel<BLOCK, MINB, TMODE, RARE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     if (e != cudaSuccess) return e;
-    attr_set[dev & 63] = true;
+    attr_set[dev & 63].store(true, std::memory_order_release);
   }
   track_kernel<BLOCK, MINB, TMODE, RARE><<<grid, BLOCK, smem, st>>>(a);
   return cudaGetLastError();

@@ -9,6 +9,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -22,6 +24,33 @@
 
 using namespace bgt;
 
+// Resources of one call.  A call takes a context from its handle's pool (a
+// new one when all are busy) and returns it when the call returns, so calls
+// that run at the same time on one handle -- from OpenMP threads, as the
+// reference calls track1 (bmad/multiparticle/beam_utils.f90:69-74) -- never
+// share a stream, staging buffers or the kernel's tile counter.  `done`
+// marks the end of the GPU work the context's last call enqueued; the next
+// call orders its own stream after it before reusing the device scratch.
+struct CallCtx {
+  cudaStream_t st = nullptr;     // library-owned stream (host-buffer calls)
+  cudaEvent_t done = nullptr;
+  bool used = false;             // `done` has been recorded
+  int32_t* d_scratch = nullptr;  // [0] tile counter, [1] error flag, [2] status read-back
+  // device staging of host-buffer calls
+  double* d_vec6 = nullptr;
+  double* d_beta = nullptr;
+  int32_t* d_i32 = nullptr;  // state, ixe, ixt, slot map, tile variant
+  int64_t cap = 0, cap_slots = 0, cap_tiles = 0;
+  // pinned host staging of host-buffer calls
+  unsigned char* h_pin = nullptr;
+  size_t pin_bytes = 0;
+  // device-buffer calls: grouping by variant (slot map, tile variant; per
+  // variant first index / count / first slot (int64) plus a check flag)
+  int32_t* d_grp = nullptr;
+  int64_t* d_grp_v = nullptr;
+  int64_t grp_cap_slots = 0, grp_cap_tiles = 0;
+};
+
 struct bgt_handle {
   int device = 0;
   int num_sms = 148;
@@ -33,25 +62,20 @@ struct bgt_handle {
   std::vector<int64_t> h_table_off;
   double* d_tables = nullptr;
   int64_t* d_table_off = nullptr;
-  int32_t* d_scratch = nullptr;  // [0] tile counter, [1] error flag
-  bgt_tuning tuning{128, 4, 0, 0, 0};
-  bool rare = false;  // some record needs the RARE kernels
-  std::string err;
-  int64_t launches = 0;
-  // host-API staging
-  double* d_vec6 = nullptr;
-  double* d_beta = nullptr;
-  int32_t* d_i32 = nullptr;  // state, ixe, ixt, slot map, tile variant
-  int64_t cap = 0, cap_slots = 0, cap_tiles = 0;
-  // device-API grouping by variant: slot map, tile variant, and per variant
-  // first index / count / first slot (int64) plus a check flag
-  int32_t* d_grp = nullptr;
-  int64_t* d_grp_v = nullptr;
-  int64_t grp_cap_slots = 0, grp_cap_tiles = 0;
+  int32_t* d_status = nullptr;  // sticky error flag of device-buffer calls (bgt_device_status)
+  bool rare = false;            // some record needs the RARE kernels
+  std::atomic<int64_t> launches{0};
+  std::mutex mu;  // guards tuning and the context pool
+  bgt_tuning tuning{128, 4, 0, 0, 0, 0, 0};
+  std::vector<CallCtx*> pool, idle;
 };
 
-static int set_err(bgt_handle* h, int code, const std::string& msg) {
-  if (h) h->err = msg;
+// Error messages are per thread: concurrent calls never overwrite each
+// other's message.
+static thread_local std::string t_err;
+
+static int set_err(bgt_handle*, int code, const std::string& msg) {
+  t_err = msg;
   return code;
 }
 
@@ -62,6 +86,87 @@ static int set_err(bgt_handle* h, int code, const std::string& msg) {
       return set_err((h), BGT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
   } while (0)
 
+// Makes `dev` current for the scope of a call and restores the caller's
+// current device on every return path.
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceGuard(int dev) {
+    if ((err = cudaGetDevice(&prev)) != cudaSuccess) return;
+    if (prev != dev) err = cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+static void free_ctx(CallCtx* c) {
+  if (!c) return;
+  if (c->st) cudaStreamDestroy(c->st);
+  if (c->done) cudaEventDestroy(c->done);
+  cudaFree(c->d_scratch);
+  cudaFree(c->d_vec6);
+  cudaFree(c->d_beta);
+  cudaFree(c->d_i32);
+  cudaFree(c->d_grp);
+  cudaFree(c->d_grp_v);
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  delete c;
+}
+
+// A context of the handle's pool for this call (the handle's device current).
+static int acquire_ctx(bgt_handle* h, CallCtx** out) {
+  *out = nullptr;
+  {
+    std::lock_guard<std::mutex> g(h->mu);
+    if (!h->idle.empty()) {
+      *out = h->idle.back();
+      h->idle.pop_back();
+      return 0;
+    }
+  }
+  CallCtx* c = new CallCtx();
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_scratch, 64)) != cudaSuccess ||
+      (e = cudaMemsetAsync(c->d_scratch, 0, 64, c->st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(c->st)) != cudaSuccess) {
+    free_ctx(c);
+    return set_err(h, BGT_ECUDA, std::string("call context: ") + cudaGetErrorString(e));
+  }
+  std::lock_guard<std::mutex> g(h->mu);
+  h->pool.push_back(c);
+  *out = c;
+  return 0;
+}
+
+// One call's lease on a context: `use(st)` orders stream st after the
+// context's previous work; the destructor marks the end of this call's work
+// on st and returns the context to the pool.
+struct CtxLease {
+  bgt_handle* h;
+  CallCtx* c = nullptr;
+  cudaStream_t st = nullptr;
+  explicit CtxLease(bgt_handle* hh) : h(hh) {}
+  int acquire() { return acquire_ctx(h, &c); }
+  cudaError_t use(cudaStream_t s) {
+    st = s;
+    return c->used && s != c->st ? cudaStreamWaitEvent(s, c->done, 0) : cudaSuccess;
+  }
+  ~CtxLease() {
+    if (!c) return;
+    if (cudaEventRecord(c->done, st ? st : c->st) == cudaSuccess) c->used = true;
+    std::lock_guard<std::mutex> g(h->mu);
+    h->idle.push_back(c);
+  }
+};
+
+static bgt_tuning get_tuning_locked(bgt_handle* h) {
+  std::lock_guard<std::mutex> g(h->mu);
+  return h->tuning;
+}
 
 static size_t smem_bytes(const bgt_handle* h, int block, bool compact, bool gtab = false) {
   size_t b = gtab ? 0 : (size_t)h->table_dw * 8;
@@ -103,37 +208,43 @@ static LaunchFn find_track_kernel(int block, int minb, int tmode, bool rare) {
 }
 
 // Fill every kernel group's copy of the multipole coefficient tables on the
-// current device.
+// current device, once per device (the values never change).
 static cudaError_t upload_multipole_tables() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
   static double cm[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1], cm0[BGT_MAXPOLE_DEV + 1][BGT_MAXPOLE_DEV + 1];
   host::c_multi_tables(cm, cm0);
-  for (int g = 0; g < N_KERNEL_GROUPS; g++) {
-    cudaError_t e = track_kernel_group(g).upload_cm(&cm[0][0], &cm0[0][0], sizeof(cm));
+  for (int gi = 0; gi < N_KERNEL_GROUPS; gi++) {
+    e = track_kernel_group(gi).upload_cm(&cm[0][0], &cm0[0][0], sizeof(cm));
     if (e != cudaSuccess) return e;
   }
+  if (dev >= 0 && dev < 64) done[dev] = true;
   return cudaSuccess;
 }
 
-// Enqueue tracking of slots on `st`.
-static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t st) {
-  int block = h->tuning.threads_per_block;
-  bool compact = a.compact_every > 0;
+// Wait bound of the staging mbarrier.
+static uint64_t wait_ns_of(const bgt_tuning& t) {
+  return t.wait_limit_us > 0 ? (uint64_t)t.wait_limit_us * 1000ull : 2000000000ull;
+}
+
+// The kernel instance for a tuning and a shared-memory need, with the
+// placement of the table it implies; 0 or an error code.
+static int pick_kernel(bgt_handle* h, const bgt_tuning& tun, bool compact, LaunchFn* fn, size_t* smem) {
+  const int block = tun.threads_per_block;
   const bool fits = smem_bytes(h, block, compact) <= SMEM_LIMIT;
-  if (h->tuning.table_mode == 1 && !fits)
+  if (tun.table_mode == 1 && !fits)
     return set_err(h, BGT_ETOOLARGE, "element table does not fit in shared memory (table_mode 1)");
-  const bool gtab = h->tuning.table_mode >= 2 || !fits;
-  const bool warp_sched = h->tuning.table_mode == 3;
-  size_t smem = smem_bytes(h, block, compact, gtab);
-  if (smem > SMEM_LIMIT) return set_err(h, BGT_ETOOLARGE, "tracking state does not fit in shared memory");
-  int64_t grid = (int64_t)h->num_sms * std::max(1, h->tuning.blocks_per_sm);
-  if (grid > n_tiles) grid = n_tiles;
-  if (grid < 1) grid = 1;
-  a.tile_counter = h->d_scratch;
-  a.error_flag = h->d_scratch + 1;
-  CU(h, cudaMemsetAsync(h->d_scratch, 0, sizeof(int32_t), st));
-  const int bps = h->tuning.blocks_per_sm;
-  const LaunchFn launch = find_track_kernel(block, bps, gtab ? (warp_sched ? 2 : 1) : 0, h->rare);
-  if (!launch) {
+  const bool gtab = tun.table_mode >= 2 || !fits;
+  const bool warp_sched = tun.table_mode == 3;
+  *smem = smem_bytes(h, block, compact, gtab);
+  if (*smem > SMEM_LIMIT) return set_err(h, BGT_ETOOLARGE, "tracking state does not fit in shared memory");
+  *fn = find_track_kernel(block, tun.blocks_per_sm, gtab ? (warp_sched ? 2 : 1) : 0, h->rare);
+  if (!*fn) {
     if (gtab)
       return set_err(h, BGT_ETOOLARGE,
                      "element table read from global memory: tuning must be (128: 3,4,5) or (256: 2,3)");
@@ -141,13 +252,32 @@ static int enqueue_track(bgt_handle* h, KArgs a, int64_t n_tiles, cudaStream_t s
                    "tuning (threads_per_block, blocks_per_sm) must be one of (64: 8,10,12,16), "
                    "(128: 4,5,6,8), (256: 2,3,4)");
   }
+  return 0;
+}
+
+// Enqueue tracking of slots on `st` with the call context's tile counter
+// and error flag.
+static int enqueue_track(bgt_handle* h, const bgt_tuning& tun, CallCtx* c, KArgs a, int64_t n_tiles,
+                         cudaStream_t st) {
+  LaunchFn launch = nullptr;
+  size_t smem = 0;
+  int rc = pick_kernel(h, tun, a.compact_every > 0, &launch, &smem);
+  if (rc) return rc;
+  int64_t grid = (int64_t)h->num_sms * std::max(1, tun.blocks_per_sm);
+  if (grid > n_tiles) grid = n_tiles;
+  if (grid < 1) grid = 1;
+  a.tile_counter = c->d_scratch;
+  a.error_flag = c->d_scratch + 1;
+  a.wait_ns = wait_ns_of(tun);
+  a.skip_table_copy = tun.test_skip_table_copy;
+  CU(h, cudaMemsetAsync(c->d_scratch, 0, sizeof(int32_t), st));
   const cudaError_t e = launch(a, (int)grid, smem, st);
   if (e != cudaSuccess) return set_err(h, BGT_ECUDA, std::string("track_kernel launch: ") + cudaGetErrorString(e));
   h->launches++;
   return 0;
 }
 
-static KArgs base_args(bgt_handle* h) {
+static KArgs base_args(bgt_handle* h, const bgt_tuning& tun) {
   KArgs a{};
   a.tables = h->d_tables;
   a.table_off_dw = h->d_table_off;
@@ -156,15 +286,30 @@ static KArgs base_args(bgt_handle* h) {
   a.rec_begin = 0;
   a.rec_end = h->n_ele;
   a.G = h->G;
-  a.compact_every = h->tuning.compact_every;
+  a.compact_every = tun.compact_every;
   return a;
+}
+
+// Tuning as bgt_set_tuning normalises it; 0 or BGT_EINVAL with the message.
+static int normalise_tuning(bgt_handle* h, bgt_tuning* n) {
+  if (n->threads_per_block == 0) n->threads_per_block = 128;
+  if (n->blocks_per_sm == 0) n->blocks_per_sm = 4;
+  if (n->threads_per_block != 64 && n->threads_per_block != 128 && n->threads_per_block != 256)
+    return set_err(h, BGT_EINVAL, "threads_per_block must be 64, 128 or 256");
+  if (n->compact_every < 0 || n->turns_per_launch < 0 || n->wait_limit_us < 0)
+    return set_err(h, BGT_EINVAL, "negative tuning value");
+  if (n->table_mode < 0 || n->table_mode > 3) return set_err(h, BGT_EINVAL, "table_mode must be 0, 1, 2 or 3");
+  if (n->test_skip_table_copy != 0 && n->test_skip_table_copy != 1)
+    return set_err(h, BGT_EINVAL, "test_skip_table_copy must be 0 or 1");
+  return 0;
 }
 
 extern "C" {
 
 int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t n_variants,
                const bgt_species* species, int32_t device) {
-  if (!out || !eles || !species || n_ele <= 0 || n_variants <= 0) return BGT_EINVAL;
+  if (!out || !eles || !species || n_ele <= 0 || n_variants <= 0)
+    return set_err(nullptr, BGT_EINVAL, "bgt_create: invalid argument");
   *out = nullptr;
   bgt_handle* h = new bgt_handle();
   h->device = device;
@@ -179,34 +324,30 @@ int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t
   h->G.ap_on = species->aperture_limit_on;
   h->G.charge = species->charge;
   std::vector<double> all;
+  std::string msg;
   int rc = host::compile_tables(eles, n_ele, n_variants, *species, QMEMO_CLASSES, all, h->h_table_off,
-                                h->table_dw, h->rare, h->err);
+                                h->table_dw, h->rare, msg);
   if (rc) {
-    std::string m = h->err;
     delete h;
     // no handle to carry the message: print it once so the caller sees why
-    fprintf(stderr, "bgt_create: %s\n", m.c_str());
-    return rc;
+    fprintf(stderr, "bgt_create: %s\n", msg.c_str());
+    return set_err(nullptr, rc, msg);
   }
   h->h_tables = all;
-  cudaError_t e;
-  if ((e = cudaSetDevice(device)) != cudaSuccess ||
+  DeviceGuard dg(device);
+  cudaError_t e = dg.err;
+  if (e != cudaSuccess ||
       (e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
       (e = cudaMalloc(&h->d_tables, all.size() * 8)) != cudaSuccess ||
       (e = cudaMalloc(&h->d_table_off, h->h_table_off.size() * 8)) != cudaSuccess ||
-      (e = cudaMalloc(&h->d_scratch, 64)) != cudaSuccess ||
+      (e = cudaMalloc(&h->d_status, 64)) != cudaSuccess ||
       (e = cudaMemcpy(h->d_tables, all.data(), all.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(h->d_table_off, h->h_table_off.data(), h->h_table_off.size() * 8, cudaMemcpyHostToDevice)) !=
           cudaSuccess ||
-      (e = cudaMemset(h->d_scratch, 0, 64)) != cudaSuccess) {
+      (e = cudaMemset(h->d_status, 0, 64)) != cudaSuccess || (e = upload_multipole_tables()) != cudaSuccess) {
     fprintf(stderr, "bgt_create: CUDA error: %s\n", cudaGetErrorString(e));
     bgt_destroy(h);
-    return BGT_ECUDA;
-  }
-  if ((e = upload_multipole_tables()) != cudaSuccess) {
-    fprintf(stderr, "bgt_create: CUDA error: %s\n", cudaGetErrorString(e));
-    bgt_destroy(h);
-    return BGT_ECUDA;
+    return set_err(nullptr, BGT_ECUDA, std::string("bgt_create: ") + cudaGetErrorString(e));
   }
   *out = h;
   return 0;
@@ -214,56 +355,53 @@ int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t
 
 int bgt_destroy(bgt_handle* h) {
   if (!h) return 0;
+  DeviceGuard dg(h->device);
+  for (CallCtx* c : h->pool) {
+    if (c->st) cudaStreamSynchronize(c->st);
+    free_ctx(c);
+  }
   cudaFree(h->d_tables);
   cudaFree(h->d_table_off);
-
-  cudaFree(h->d_scratch);
-  cudaFree(h->d_vec6);
-  cudaFree(h->d_beta);
-  cudaFree(h->d_i32);
-  cudaFree(h->d_grp);
-  cudaFree(h->d_grp_v);
+  cudaFree(h->d_status);
   delete h;
   return 0;
 }
 
-const char* bgt_last_error(const bgt_handle* h) { return h ? h->err.c_str() : "null handle"; }
+const char* bgt_last_error(const bgt_handle*) { return t_err.c_str(); }
 
 int bgt_table_info(const bgt_handle* h, int64_t* table_bytes, int32_t* n_records) {
-  if (!h) return BGT_EINVAL;
+  if (!h) return set_err(nullptr, BGT_EINVAL, "null handle");
   if (table_bytes) *table_bytes = (int64_t)h->table_dw * 8;
   if (n_records) *n_records = h->n_ele;
   return 0;
 }
 
 int bgt_set_tuning(bgt_handle* h, const bgt_tuning* t) {
-  if (!h || !t) return BGT_EINVAL;
+  if (!h || !t) return set_err(h, BGT_EINVAL, "bgt_set_tuning: invalid argument");
   bgt_tuning n = *t;
-  if (n.threads_per_block == 0) n.threads_per_block = 128;
-  if (n.blocks_per_sm == 0) n.blocks_per_sm = 4;
-  if (n.threads_per_block != 64 && n.threads_per_block != 128 && n.threads_per_block != 256)
-    return set_err(h, BGT_EINVAL, "threads_per_block must be 64, 128 or 256");
-  if (n.compact_every < 0 || n.turns_per_launch < 0) return set_err(h, BGT_EINVAL, "negative tuning value");
-  if (n.table_mode < 0 || n.table_mode > 3) return set_err(h, BGT_EINVAL, "table_mode must be 0, 1, 2 or 3");
+  int rc = normalise_tuning(h, &n);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(h->mu);
   h->tuning = n;
   return 0;
 }
 
 int bgt_get_tuning(const bgt_handle* h, bgt_tuning* t) {
-  if (!h || !t) return BGT_EINVAL;
-  *t = h->tuning;
+  if (!h || !t) return set_err(nullptr, BGT_EINVAL, "bgt_get_tuning: invalid argument");
+  *t = get_tuning_locked(const_cast<bgt_handle*>(h));
   return 0;
 }
 
-int64_t bgt_kernel_launch_count(const bgt_handle* h) { return h ? h->launches : -1; }
+int64_t bgt_kernel_launch_count(const bgt_handle* h) { return h ? h->launches.load() : -1; }
 
 // Track device-resident particles for turns [turn0, turn0 + n_turns) in
 // segments of tuning.turns_per_launch turns (one persistent launch each).
-static int track_device_impl(bgt_handle* h, double* d_vec6, int64_t n_stride, double* d_beta, int32_t* d_state,
-                             int32_t* d_ixe, int32_t* d_ixt, const int32_t* d_slot, const int32_t* d_tile_var,
-                             int64_t n, int64_t n_slots, int32_t turn0, int32_t n_turns, int32_t rec_begin,
-                             int32_t rec_end, cudaStream_t st) {
-  KArgs a = base_args(h);
+// The call's error flag is cleared once, the tile counter per launch.
+static int track_device_impl(bgt_handle* h, const bgt_tuning& tun, CallCtx* c, int32_t* status, double* d_vec6,
+                             int64_t n_stride, double* d_beta, int32_t* d_state, int32_t* d_ixe, int32_t* d_ixt,
+                             const int32_t* d_slot, const int32_t* d_tile_var, int64_t n, int64_t n_slots,
+                             int32_t turn0, int32_t n_turns, int32_t rec_begin, int32_t rec_end, cudaStream_t st) {
+  KArgs a = base_args(h, tun);
   a.vec6 = d_vec6;
   a.n_stride = n_stride;
   a.beta = d_beta;
@@ -276,12 +414,14 @@ static int track_device_impl(bgt_handle* h, double* d_vec6, int64_t n_stride, do
   a.n_slots = n_slots;
   a.rec_begin = rec_begin;
   a.rec_end = rec_end;
-  int64_t n_tiles = (n_slots + h->tuning.threads_per_block - 1) / h->tuning.threads_per_block;
-  int32_t seg = h->tuning.turns_per_launch > 0 ? h->tuning.turns_per_launch : n_turns;
+  a.status = status;
+  CU(h, cudaMemsetAsync(c->d_scratch + 1, 0, sizeof(int32_t), st));
+  int64_t n_tiles = (n_slots + tun.threads_per_block - 1) / tun.threads_per_block;
+  int32_t seg = tun.turns_per_launch > 0 ? tun.turns_per_launch : n_turns;
   for (int32_t t = 0; t < n_turns; t += seg) {
     a.turn0 = turn0 + t;
     a.n_turns = std::min(seg, n_turns - t);
-    int rc = enqueue_track(h, a, n_tiles, st);
+    int rc = enqueue_track(h, tun, c, a, n_tiles, st);
     if (rc) return rc;
   }
   return 0;
@@ -315,20 +455,28 @@ __global__ void variant_slot_kernel(const int32_t* var, int64_t n, const int64_t
 int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state, int32_t* d_ix_ele_lost,
                            int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n, int32_t turn0,
                            int32_t n_turns, void* stream) {
-  if (!h || !d_vec6 || !d_beta || !d_state || !d_ix_ele_lost || n < 0 || n_turns < 0) return BGT_EINVAL;
+  if (!h || !d_vec6 || !d_beta || !d_state || !d_ix_ele_lost || n < 0 || n_turns < 0)
+    return set_err(h, BGT_EINVAL, "bgt_track_turns_device: invalid argument");
   if (n == 0 || n_turns == 0) return 0;
   if (n > INT32_MAX) return set_err(h, BGT_EINVAL, "bgt_track_turns_device: n exceeds 2^31 - 1");
-  CU(h, cudaSetDevice(h->device));
+  DeviceGuard dg(h->device);
+  CU(h, dg.err);
+  const bgt_tuning tun = get_tuning_locked(h);
   cudaStream_t st = (cudaStream_t)stream;
+  CtxLease L(h);
+  int rc = L.acquire();
+  if (rc) return rc;
+  CallCtx* c = L.c;
+  CU(h, L.use(st));
   if (!d_variant || h->n_variants == 1)
-    return track_device_impl(h, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost, nullptr, nullptr, n, n,
-                             turn0, n_turns, 0, h->n_ele, st);
+    return track_device_impl(h, tun, c, h->d_status, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost,
+                             nullptr, nullptr, n, n, turn0, n_turns, 0, h->n_ele, st);
   // Group by variant into tile-aligned slot ranges.  The variant ids must be
   // sorted (non-decreasing); the per-variant counts are read back once.
   const int32_t nv = h->n_variants;
-  const int block = h->tuning.threads_per_block;
-  if (!h->d_grp_v) CU(h, cudaMalloc(&h->d_grp_v, ((size_t)3 * nv + 1) * 8));
-  int64_t* d_first = h->d_grp_v;
+  const int block = tun.threads_per_block;
+  if (!c->d_grp_v) CU(h, cudaMalloc(&c->d_grp_v, ((size_t)3 * nv + 1) * 8));
+  int64_t* d_first = c->d_grp_v;
   int64_t* d_count = d_first + nv;
   int64_t* d_slot0 = d_count + nv;
   int32_t* d_bad = (int32_t*)(d_slot0 + nv);
@@ -352,16 +500,16 @@ int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_
     s += tiles * block;
   }
   const int64_t n_slots = s, n_tiles = (int64_t)tvar.size();
-  if (n_slots > h->grp_cap_slots || n_tiles > h->grp_cap_tiles) {
+  if (n_slots > c->grp_cap_slots || n_tiles > c->grp_cap_tiles) {
     CU(h, cudaStreamSynchronize(st));
-    cudaFree(h->d_grp);
-    h->d_grp = nullptr;
-    h->grp_cap_slots = std::max(n_slots, h->grp_cap_slots);
-    h->grp_cap_tiles = std::max(n_tiles, h->grp_cap_tiles);
-    CU(h, cudaMalloc(&h->d_grp, (size_t)(h->grp_cap_slots + h->grp_cap_tiles) * 4));
+    cudaFree(c->d_grp);
+    c->d_grp = nullptr;
+    c->grp_cap_slots = std::max(n_slots, c->grp_cap_slots);
+    c->grp_cap_tiles = std::max(n_tiles, c->grp_cap_tiles);
+    CU(h, cudaMalloc(&c->d_grp, (size_t)(c->grp_cap_slots + c->grp_cap_tiles) * 4));
   }
-  int32_t* d_slot = h->d_grp;
-  int32_t* d_tvar = d_slot + h->grp_cap_slots;
+  int32_t* d_slot = c->d_grp;
+  int32_t* d_tvar = d_slot + c->grp_cap_slots;
   CU(h, cudaMemcpyAsync(d_slot0, slot0.data(), (size_t)nv * 8, cudaMemcpyHostToDevice, st));
   CU(h, cudaMemcpyAsync(d_tvar, tvar.data(), (size_t)n_tiles * 4, cudaMemcpyHostToDevice, st));
   CU(h, cudaMemsetAsync(d_slot, 0xff, (size_t)n_slots * 4, st));
@@ -369,36 +517,75 @@ int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_
   h->launches++;
   // (copies from pageable host memory return once the data is staged, so
   // slot0 and tvar may go out of scope before the copies complete)
-  return track_device_impl(h, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost, d_slot, d_tvar, n, n_slots,
-                           turn0, n_turns, 0, h->n_ele, st);
+  return track_device_impl(h, tun, c, h->d_status, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost,
+                           d_slot, d_tvar, n, n_slots, turn0, n_turns, 0, h->n_ele, st);
 }
 
-// Grow the host-API staging buffers.
-static int ensure_staging(bgt_handle* h, int64_t n, int64_t n_slots, int64_t n_tiles) {
-  if (n <= h->cap && n_slots <= h->cap_slots && n_tiles <= h->cap_tiles) return 0;
-  cudaFree(h->d_vec6);
-  cudaFree(h->d_beta);
-  cudaFree(h->d_i32);
-  h->d_vec6 = nullptr;
-  h->d_beta = nullptr;
-  h->d_i32 = nullptr;
-  h->cap = std::max(n, h->cap);
-  h->cap_slots = std::max(n_slots, h->cap_slots);
-  h->cap_tiles = std::max(n_tiles, h->cap_tiles);
-  CU(h, cudaMalloc(&h->d_vec6, (size_t)h->cap * 6 * 8));
-  CU(h, cudaMalloc(&h->d_beta, (size_t)h->cap * 8));
-  CU(h, cudaMalloc(&h->d_i32, (size_t)(3 * h->cap + h->cap_slots + h->cap_tiles) * 4));
+// Reads and clears the handle's device error flag after `stream` completes.
+__global__ void take_status_kernel(int32_t* status, int32_t* out) { *out = atomicExch(status, 0); }
+
+int bgt_device_status(bgt_handle* h, void* stream) {
+  if (!h) return set_err(nullptr, BGT_EINVAL, "null handle");
+  DeviceGuard dg(h->device);
+  CU(h, dg.err);
+  cudaStream_t st = (cudaStream_t)stream;
+  CtxLease L(h);
+  int rc = L.acquire();
+  if (rc) return rc;
+  CU(h, L.use(st));
+  take_status_kernel<<<1, 1, 0, st>>>(h->d_status, L.c->d_scratch + 2);
+  h->launches++;
+  int32_t flag = 0;
+  CU(h, cudaMemcpyAsync(&flag, L.c->d_scratch + 2, 4, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaStreamSynchronize(st));
+  if (flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete on the device");
   return 0;
 }
 
-// Host-buffer tracking shared by bgt_track_turns and bgt_track_elements.
+// Grow a context's device staging buffers.
+static int ensure_staging(bgt_handle* h, CallCtx* c, int64_t n, int64_t n_slots, int64_t n_tiles) {
+  if (n <= c->cap && n_slots <= c->cap_slots && n_tiles <= c->cap_tiles) return 0;
+  CU(h, cudaStreamSynchronize(c->st));
+  cudaFree(c->d_vec6);
+  cudaFree(c->d_beta);
+  cudaFree(c->d_i32);
+  c->d_vec6 = nullptr;
+  c->d_beta = nullptr;
+  c->d_i32 = nullptr;
+  c->cap = std::max(n, c->cap);
+  c->cap_slots = std::max(n_slots, c->cap_slots);
+  c->cap_tiles = std::max(n_tiles, c->cap_tiles);
+  CU(h, cudaMalloc(&c->d_vec6, (size_t)c->cap * 6 * 8));
+  CU(h, cudaMalloc(&c->d_beta, (size_t)c->cap * 8));
+  CU(h, cudaMalloc(&c->d_i32, (size_t)(3 * c->cap + c->cap_slots + c->cap_tiles) * 4));
+  return 0;
+}
+
+// Grow a context's pinned host staging buffer.
+static int ensure_pinned(bgt_handle* h, CallCtx* c, size_t bytes) {
+  if (bytes <= c->pin_bytes) return 0;
+  CU(h, cudaStreamSynchronize(c->st));
+  if (c->h_pin) cudaFreeHost(c->h_pin);
+  c->h_pin = nullptr;
+  c->pin_bytes = 0;
+  CU(h, cudaMallocHost(&c->h_pin, bytes));
+  c->pin_bytes = bytes;
+  return 0;
+}
+
+// Host-buffer tracking shared by bgt_track_turns and bgt_track_elements: the
+// particles go through the context's pinned staging buffer to its device
+// buffers on its own stream; the call waits for that stream only.
 static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ixe, int32_t* ixt,
                       const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns, int32_t rec_begin,
                       int32_t rec_end) {
-  if (!h || !vec6 || !beta || !state || !ixe || n < 0) return BGT_EINVAL;
+  if (!h || !vec6 || !beta || !state || !ixe || n < 0) return set_err(h, BGT_EINVAL, "invalid argument");
   if (n == 0 || n_turns == 0) return 0;
-  CU(h, cudaSetDevice(h->device));
-  const int block = h->tuning.threads_per_block;
+  if (n > INT32_MAX) return set_err(h, BGT_EINVAL, "n exceeds 2^31 - 1");
+  DeviceGuard dg(h->device);
+  CU(h, dg.err);
+  const bgt_tuning tun = get_tuning_locked(h);
+  const int block = tun.threads_per_block;
   // group particles by variant into tile-aligned slot ranges
   std::vector<int32_t> slot_map, tile_var;
   int64_t n_slots = n;
@@ -421,52 +608,87 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
     slot_map.assign(n_slots, -1);
     std::vector<int64_t> fill = start;
     for (int64_t i = 0; i < n; i++) slot_map[fill[variant[i]]++] = (int32_t)i;
-  }
-  int64_t n_tiles = (n_slots + block - 1) / block;
-  int rc = ensure_staging(h, n, n_slots, n_tiles);
-  if (rc) return rc;
-  int32_t* d_state = h->d_i32;
-  int32_t* d_ixe = d_state + h->cap;
-  int32_t* d_ixt = d_ixe + h->cap;
-  int32_t* d_slot = d_ixt + h->cap;
-  int32_t* d_tvar = d_slot + h->cap_slots;
-  CU(h, cudaMemcpy2D(h->d_vec6, h->cap * 8, vec6, n * 8, n * 8, 6, cudaMemcpyHostToDevice));
-  CU(h, cudaMemcpy(h->d_beta, beta, n * 8, cudaMemcpyHostToDevice));
-  CU(h, cudaMemcpy(d_state, state, n * 4, cudaMemcpyHostToDevice));
-  CU(h, cudaMemcpy(d_ixe, ixe, n * 4, cudaMemcpyHostToDevice));
-  if (ixt) CU(h, cudaMemcpy(d_ixt, ixt, n * 4, cudaMemcpyHostToDevice));
-  if (multi) {
-    CU(h, cudaMemcpy(d_slot, slot_map.data(), n_slots * 4, cudaMemcpyHostToDevice));
-    CU(h, cudaMemcpy(d_tvar, tile_var.data(), tile_var.size() * 4, cudaMemcpyHostToDevice));
   } else if (variant && h->n_variants == 1) {
     for (int64_t i = 0; i < n; i++)
       if (variant[i] != 0) return set_err(h, BGT_EINVAL, "variant out of range");
   }
-  rc = track_device_impl(h, h->d_vec6, h->cap, h->d_beta, d_state, d_ixe, ixt ? d_ixt : nullptr,
-                         multi ? d_slot : nullptr, multi ? d_tvar : nullptr, n, n_slots, turn0, n_turns, rec_begin,
-                         rec_end, 0);
+  int64_t n_tiles = (n_slots + block - 1) / block;
+  CtxLease L(h);
+  int rc = L.acquire();
   if (rc) return rc;
-  CU(h, cudaDeviceSynchronize());
-  int32_t flag = 0;
-  CU(h, cudaMemcpy(&flag, h->d_scratch + 1, 4, cudaMemcpyDeviceToHost));
-  if (flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete");
-  CU(h, cudaMemcpy2D(vec6, n * 8, h->d_vec6, h->cap * 8, n * 8, 6, cudaMemcpyDeviceToHost));
-  CU(h, cudaMemcpy(beta, h->d_beta, n * 8, cudaMemcpyDeviceToHost));
-  CU(h, cudaMemcpy(state, d_state, n * 4, cudaMemcpyDeviceToHost));
-  CU(h, cudaMemcpy(ixe, d_ixe, n * 4, cudaMemcpyDeviceToHost));
-  if (ixt) CU(h, cudaMemcpy(ixt, d_ixt, n * 4, cudaMemcpyDeviceToHost));
+  CallCtx* c = L.c;
+  cudaStream_t st = c->st;
+  CU(h, L.use(st));
+  if ((rc = ensure_staging(h, c, n, n_slots, n_tiles))) return rc;
+  // pinned layout: vec6 [6][n], beta [n], state/ixe/ixt [n] each, slot map,
+  // tile variants, error flag
+  const size_t b_v = (size_t)n * 6 * 8, b_b = (size_t)n * 8, b_i = (size_t)n * 4;
+  const size_t b_slot = multi ? (size_t)n_slots * 4 : 0, b_tv = multi ? tile_var.size() * 4 : 0;
+  if ((rc = ensure_pinned(h, c, b_v + b_b + 3 * b_i + b_slot + b_tv + 16))) return rc;
+  unsigned char* p = c->h_pin;
+  double* p_v = (double*)p;
+  double* p_b = (double*)(p + b_v);
+  int32_t* p_s = (int32_t*)(p + b_v + b_b);
+  int32_t* p_e = p_s + n;
+  int32_t* p_t = p_e + n;
+  int32_t* p_slot = p_t + n;
+  int32_t* p_tv = p_slot + (multi ? n_slots : 0);
+  int32_t* p_flag = p_tv + (multi ? tile_var.size() : 0);
+  memcpy(p_v, vec6, b_v);
+  memcpy(p_b, beta, b_b);
+  memcpy(p_s, state, b_i);
+  memcpy(p_e, ixe, b_i);
+  if (ixt) memcpy(p_t, ixt, b_i);
+  if (multi) {
+    memcpy(p_slot, slot_map.data(), b_slot);
+    memcpy(p_tv, tile_var.data(), b_tv);
+  }
+  int32_t* d_state = c->d_i32;
+  int32_t* d_ixe = d_state + c->cap;
+  int32_t* d_ixt = d_ixe + c->cap;
+  int32_t* d_slot = d_ixt + c->cap;
+  int32_t* d_tvar = d_slot + c->cap_slots;
+  CU(h, cudaMemcpy2DAsync(c->d_vec6, c->cap * 8, p_v, n * 8, n * 8, 6, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemcpyAsync(c->d_beta, p_b, b_b, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemcpyAsync(d_state, p_s, b_i, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemcpyAsync(d_ixe, p_e, b_i, cudaMemcpyHostToDevice, st));
+  if (ixt) CU(h, cudaMemcpyAsync(d_ixt, p_t, b_i, cudaMemcpyHostToDevice, st));
+  if (multi) {
+    CU(h, cudaMemcpyAsync(d_slot, p_slot, b_slot, cudaMemcpyHostToDevice, st));
+    CU(h, cudaMemcpyAsync(d_tvar, p_tv, b_tv, cudaMemcpyHostToDevice, st));
+  }
+  rc = track_device_impl(h, tun, c, nullptr, c->d_vec6, c->cap, c->d_beta, d_state, d_ixe, ixt ? d_ixt : nullptr,
+                         multi ? d_slot : nullptr, multi ? d_tvar : nullptr, n, n_slots, turn0, n_turns, rec_begin,
+                         rec_end, st);
+  if (rc) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
+  CU(h, cudaMemcpyAsync(p_flag, c->d_scratch + 1, 4, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaMemcpy2DAsync(p_v, n * 8, c->d_vec6, c->cap * 8, n * 8, 6, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaMemcpyAsync(p_b, c->d_beta, b_b, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaMemcpyAsync(p_s, d_state, b_i, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaMemcpyAsync(p_e, d_ixe, b_i, cudaMemcpyDeviceToHost, st));
+  if (ixt) CU(h, cudaMemcpyAsync(p_t, d_ixt, b_i, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaStreamSynchronize(st));
+  if (*p_flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete");
+  memcpy(vec6, p_v, b_v);
+  memcpy(beta, p_b, b_b);
+  memcpy(state, p_s, b_i);
+  memcpy(ixe, p_e, b_i);
+  if (ixt) memcpy(ixt, p_t, b_i);
   return 0;
 }
 
 int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
                     int32_t* ix_turn_lost, const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns) {
-  if (!h) return BGT_EINVAL;
+  if (!h) return set_err(nullptr, BGT_EINVAL, "null handle");
   return track_host(h, vec6, beta, state, ix_ele_lost, ix_turn_lost, variant, n, turn0, n_turns, 0, h->n_ele);
 }
 
 int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
                        const int32_t* variant, int64_t n, int32_t e_begin, int32_t e_end) {
-  if (!h) return BGT_EINVAL;
+  if (!h) return set_err(nullptr, BGT_EINVAL, "null handle");
   if (e_begin < 0 || e_end > h->n_ele || e_begin >= e_end) return set_err(h, BGT_EINVAL, "bad element range");
   return track_host(h, vec6, beta, state, ix_ele_lost, nullptr, variant, n, 0, 1, e_begin, e_end);
 }
@@ -573,15 +795,16 @@ __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
 
 extern "C" {
 
-int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_used, const double* deltas,
-                     int32_t n_delta, int32_t n_angle, double angle_min, double angle_max, int32_t n_radius,
-                     double r_max, double y_scale, int32_t n_turns, double* da_radius, int32_t* survive_turns) {
-  (void)deltas;
+int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_used, int32_t n_delta,
+                     int32_t n_angle, double angle_min, double angle_max, int32_t n_radius, double r_max,
+                     double y_scale, int32_t n_turns, double* da_radius, int32_t* survive_turns) {
   if (!h || !ref_orbit || !da_radius || n_variants_used <= 0 || n_variants_used > h->n_variants || n_delta <= 0 ||
       n_angle <= 0 || n_radius <= 1 || n_turns <= 0)
-    return BGT_EINVAL;
-  CU(h, cudaSetDevice(h->device));
-  const int block = h->tuning.threads_per_block;
+    return set_err(h, BGT_EINVAL, "bgt_da_scan_grid: invalid argument");
+  DeviceGuard dg(h->device);
+  CU(h, dg.err);
+  const bgt_tuning tun = get_tuning_locked(h);
+  const int block = tun.threads_per_block;
   DAArgs A{};
   A.n_var = n_variants_used;
   A.n_delta = n_delta;
@@ -597,18 +820,21 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
   int64_t n = A.per_var * n_variants_used;
   int64_t n_slots = A.slots_per_var * n_variants_used;
   int64_t n_tiles = tiles_per_var * n_variants_used;
+  if (n > INT32_MAX) return set_err(h, BGT_EINVAL, "bgt_da_scan_grid: more than 2^31 - 1 probes");
   A.p0c = h->G.p0c;
   A.mc2 = h->G.mc2;
-  int rc = ensure_staging(h, n, n_slots, n_tiles);
+  CtxLease L(h);
+  int rc = L.acquire();
   if (rc) return rc;
-  int32_t* d_state = h->d_i32;
-  int32_t* d_ixe = d_state + h->cap;
-  int32_t* d_ixt = d_ixe + h->cap;
-  int32_t* d_slot = d_ixt + h->cap;
-  int32_t* d_tvar = d_slot + h->cap_slots;
-  double* d_ref = nullptr;
-  double* d_da = nullptr;
-  int32_t* d_surv = nullptr;
+  CallCtx* c = L.c;
+  cudaStream_t st = c->st;
+  CU(h, L.use(st));
+  if ((rc = ensure_staging(h, c, n, n_slots, n_tiles))) return rc;
+  int32_t* d_state = c->d_i32;
+  int32_t* d_ixe = d_state + c->cap;
+  int32_t* d_ixt = d_ixe + c->cap;
+  int32_t* d_slot = d_ixt + c->cap;
+  int32_t* d_tvar = d_slot + c->cap_slots;
   int64_t n_rays = (int64_t)n_variants_used * n_delta * n_angle;
   // ray directions: angle_j = j * delta_angle + min_angle
   // (dynamic_aperture_mod.f90:88-95), cos/sin by the host C library
@@ -618,48 +844,51 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
     cs[2 * j] = cos(ang);
     cs[2 * j + 1] = sin(ang);
   }
-  double* d_cs = nullptr;
-  CU(h, cudaMalloc(&d_cs, cs.size() * 8));
-  CU(h, cudaMemcpy(d_cs, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice));
+  // per-call device buffers: ray directions, reference orbits, radii,
+  // survival turns (one allocation)
+  const size_t b_cs = cs.size() * 8, b_ref = (size_t)n_variants_used * n_delta * 6 * 8, b_da = (size_t)n_rays * 8;
+  const size_t b_surv = survive_turns ? (size_t)n * 4 : 0;
+  unsigned char* d_buf = nullptr;
+  CU(h, cudaMalloc(&d_buf, b_cs + b_ref + b_da + b_surv));
+  struct Free {
+    unsigned char* p;
+    cudaStream_t st;
+    ~Free() {
+      cudaStreamSynchronize(st);
+      cudaFree(p);
+    }
+  } free_buf{d_buf, st};
+  double* d_cs = (double*)d_buf;
+  double* d_ref = (double*)(d_buf + b_cs);
+  double* d_da = (double*)(d_buf + b_cs + b_ref);
+  int32_t* d_surv = survive_turns ? (int32_t*)(d_buf + b_cs + b_ref + b_da) : nullptr;
+  CU(h, cudaMemcpyAsync(d_cs, cs.data(), b_cs, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemcpyAsync(d_ref, ref_orbit, b_ref, cudaMemcpyHostToDevice, st));
+  CU(h, cudaMemsetAsync(d_slot, 0xff, (size_t)n_slots * 4, st));
   A.cs = d_cs;
-  CU(h, cudaMalloc(&d_ref, (size_t)n_variants_used * n_delta * 6 * 8));
-  CU(h, cudaMalloc(&d_da, (size_t)n_rays * 8));
-  if (survive_turns) CU(h, cudaMalloc(&d_surv, (size_t)n * 4));
-  CU(h, cudaMemcpy(d_ref, ref_orbit, (size_t)n_variants_used * n_delta * 6 * 8, cudaMemcpyHostToDevice));
-  CU(h, cudaMemset(d_slot, 0xff, (size_t)n_slots * 4));
   A.ref = d_ref;
-  A.vec6 = h->d_vec6;
-  A.stride = h->cap;
-  A.beta = h->d_beta;
+  A.vec6 = c->d_vec6;
+  A.stride = c->cap;
+  A.beta = c->d_beta;
   A.state = d_state;
   A.ixe = d_ixe;
   A.ixt = d_ixt;
   A.slot = d_slot;
   A.block = block;
-  da_init_kernel<<<(unsigned)((n + 255) / 256), 256>>>(A, n);
-  da_tile_var_kernel<<<(unsigned)((n_tiles + 255) / 256), 256>>>(d_tvar, tiles_per_var, n_tiles);
+  da_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A, n);
+  da_tile_var_kernel<<<(unsigned)((n_tiles + 255) / 256), 256, 0, st>>>(d_tvar, tiles_per_var, n_tiles);
   h->launches += 2;
-  rc = track_device_impl(h, h->d_vec6, h->cap, h->d_beta, d_state, d_ixe, d_ixt, d_slot, d_tvar, n, n_slots, 0,
-                         n_turns, 0, h->n_ele, 0);
-  if (rc) {
-    cudaFree(d_ref);
-    cudaFree(d_da);
-    cudaFree(d_surv);
-    cudaFree(d_cs);
-    return rc;
-  }
-  da_reduce_kernel<<<(unsigned)((n_rays + 127) / 128), 128>>>(d_state, d_ixt, n_rays, n_radius, A.dr, 0, n_turns,
-                                                              d_da, d_surv);
+  rc = track_device_impl(h, tun, c, nullptr, c->d_vec6, c->cap, c->d_beta, d_state, d_ixe, d_ixt, d_slot, d_tvar, n,
+                         n_slots, 0, n_turns, 0, h->n_ele, st);
+  if (rc) return rc;
+  da_reduce_kernel<<<(unsigned)((n_rays + 127) / 128), 128, 0, st>>>(d_state, d_ixt, n_rays, n_radius, A.dr, 0,
+                                                                     n_turns, d_da, d_surv);
   h->launches++;
-  CU(h, cudaDeviceSynchronize());
   int32_t flag = 0;
-  CU(h, cudaMemcpy(&flag, h->d_scratch + 1, 4, cudaMemcpyDeviceToHost));
-  CU(h, cudaMemcpy(da_radius, d_da, (size_t)n_rays * 8, cudaMemcpyDeviceToHost));
-  if (survive_turns) CU(h, cudaMemcpy(survive_turns, d_surv, (size_t)n * 4, cudaMemcpyDeviceToHost));
-  cudaFree(d_ref);
-  cudaFree(d_da);
-  cudaFree(d_surv);
-  cudaFree(d_cs);
+  CU(h, cudaMemcpyAsync(&flag, c->d_scratch + 1, 4, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaMemcpyAsync(da_radius, d_da, b_da, cudaMemcpyDeviceToHost, st));
+  if (survive_turns) CU(h, cudaMemcpyAsync(survive_turns, d_surv, b_surv, cudaMemcpyDeviceToHost, st));
+  CU(h, cudaStreamSynchronize(st));
   if (flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete");
   return 0;
 }
@@ -712,19 +941,22 @@ int bgt_fp64_peak_tflops(int32_t device, double* tflops) {
 // Every call uses the same array and leaves its contents behind: calls that
 // overlap on the GPU (different streams, or threads) race and must be
 // serialised by the caller.  The first call on a device resolves the array's
-// address (cudaGetSymbolAddress) and uploads the multipole coefficient
-// tables; make that first call before any stream capture.
+// address (cudaGetSymbolAddress), zeroes its header and uploads the
+// multipole coefficient tables; make that first call before any stream
+// capture.
 
 #define BGT_NOALLOC_SCRATCH_BYTES (256 * 1024)
 
 namespace bgt {
 
-// [0..15]: tile counter (int32), error flag (int32); table from byte 256 on
+// [0..3] tile counter, [4..7] error flag (int32); [16..23] table offset of
+// the single variant (int64, always 0); table from byte 256 on
 static __device__ __align__(256) unsigned char g_noalloc_scratch[BGT_NOALLOC_SCRATCH_BYTES];
 
 namespace {
 constexpr int kNoallocMaxDevices = 64;
-unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};
+std::atomic<unsigned char*> g_noalloc_ptr[kNoallocMaxDevices];
+std::mutex g_noalloc_setup_mu;
 }  // namespace
 
 }  // namespace bgt
@@ -733,7 +965,8 @@ extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n
                                               double* d_vec6, double* d_beta, int32_t* d_state,
                                               int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, int64_t n,
                                               int32_t turn0, int32_t n_turns, const bgt_tuning* tuning,
-                                              int32_t device, void* stream, char* err, int32_t err_len) {
+                                              int32_t device, void* stream, int32_t* d_status, char* err,
+                                              int32_t err_len) {
   auto fail = [&](int code, const std::string& msg) {
     if (err && err_len > 0) {
       snprintf(err, (size_t)err_len, "%s", msg.c_str());
@@ -743,20 +976,36 @@ extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n
   if (!eles || !species || n_ele <= 0 || !d_vec6 || !d_beta || !d_state || !d_ix_ele_lost || n < 0 ||
       n_turns < 0 || device < 0 || device >= bgt::kNoallocMaxDevices)
     return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: invalid argument");
+  if (n > INT32_MAX) return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: n exceeds 2^31 - 1");
+  // the launch shape is checked before anything is enqueued
+  bgt_tuning t = tuning ? *tuning : bgt_tuning{128, 4, 0, 0, 0, 0, 0};
+  if (t.threads_per_block == 0) t.threads_per_block = 128;
+  if (t.blocks_per_sm == 0) t.blocks_per_sm = 4;
+  if (!((t.threads_per_block == 128 && t.blocks_per_sm == 4) || (t.threads_per_block == 256 && t.blocks_per_sm == 2)))
+    return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: tuning must be (128, 4) or (256, 2)");
+  if (t.compact_every < 0 || t.turns_per_launch < 0 || t.wait_limit_us < 0 ||
+      (t.test_skip_table_copy != 0 && t.test_skip_table_copy != 1))
+    return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: invalid tuning value");
   if (n == 0 || n_turns == 0) return 0;
-  cudaError_t ce = cudaSetDevice(device);
+  DeviceGuard dg(device);
+  cudaError_t ce = dg.err;
   if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
 
   // one-time set-up on this device (this device current)
-  if (!bgt::g_noalloc_ptr[device]) {
-    void* p = nullptr;
-    ce = cudaGetSymbolAddress(&p, bgt::g_noalloc_scratch);
-    if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
-    if ((ce = upload_multipole_tables()) != cudaSuccess)
-      return fail(BGT_ECUDA, std::string("coefficient upload: ") + cudaGetErrorString(ce));
-    bgt::g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+  if (!bgt::g_noalloc_ptr[device].load(std::memory_order_acquire)) {
+    std::lock_guard<std::mutex> g(bgt::g_noalloc_setup_mu);
+    if (!bgt::g_noalloc_ptr[device].load(std::memory_order_acquire)) {
+      void* p = nullptr;
+      ce = cudaGetSymbolAddress(&p, bgt::g_noalloc_scratch);
+      if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce));
+      if ((ce = cudaMemset(p, 0, 256)) != cudaSuccess)
+        return fail(BGT_ECUDA, std::string("scratch header: ") + cudaGetErrorString(ce));
+      if ((ce = upload_multipole_tables()) != cudaSuccess)
+        return fail(BGT_ECUDA, std::string("coefficient upload: ") + cudaGetErrorString(ce));
+      bgt::g_noalloc_ptr[device].store(static_cast<unsigned char*>(p), std::memory_order_release);
+    }
   }
-  unsigned char* base = bgt::g_noalloc_ptr[device];
+  unsigned char* base = bgt::g_noalloc_ptr[device].load(std::memory_order_acquire);
 
   // compile the table on the host (same records as bgt_create, one variant)
   std::vector<double> tab((size_t)(n_ele + (n_ele % 2)), 0.0);
@@ -792,21 +1041,27 @@ extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n
     return fail(BGT_ETOOLARGE, "bgt_track_turns_device_noalloc: element table needs " +
                                    std::to_string(table_bytes) + " bytes, the scratch array holds " +
                                    std::to_string(BGT_NOALLOC_SCRATCH_BYTES - 256));
+  // The table is staged in shared memory when it fits, else read in place
+  // from the scratch array (global memory, CTA tiles), as bgt_create's
+  // tables are.
+  const int block = t.threads_per_block;
+  const size_t state_smem = (t.compact_every > 0 ? (size_t)9 * block * 8 : 0) +
+                            (size_t)bgt::QMEMO_CLASSES * 13 * block * 8;
+  const bool gtab = state_smem + table_bytes > SMEM_LIMIT;
+  const size_t smem = state_smem + (gtab ? 0 : table_bytes);
+  const LaunchFn launch = find_track_kernel(block, t.blocks_per_sm, gtab ? 1 : 0, rare);
+  if (!launch) return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: no kernel instance for this tuning");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+
   cudaStream_t st = (cudaStream_t)stream;
   int32_t* d_counter = reinterpret_cast<int32_t*>(base);
   double* d_table = reinterpret_cast<double*>(base + 256);
-  // table offset 0 for the single variant, kept in the scratch header
   int64_t* d_table_off = reinterpret_cast<int64_t*>(base + 16);
-  const int64_t zero_off = 0;
-  if ((ce = cudaMemcpyAsync(d_table, tab.data(), table_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (ce = cudaMemcpyAsync(d_table_off, &zero_off, sizeof(zero_off), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+  // (a copy from pageable host memory returns once the data is staged, so
+  // `tab` may go out of scope before the copy completes)
+  if ((ce = cudaMemcpyAsync(d_table, tab.data(), table_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return fail(BGT_ECUDA, std::string("table upload: ") + cudaGetErrorString(ce));
-
-  bgt_tuning t = tuning ? *tuning : bgt_tuning{128, 4, 0, 0};
-  if (t.threads_per_block == 0) t.threads_per_block = 128;
-  if (t.blocks_per_sm == 0) t.blocks_per_sm = 4;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
 
   bgt::KArgs a{};
   a.vec6 = d_vec6;
@@ -826,20 +1081,19 @@ extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n
   a.compact_every = t.compact_every;
   a.tile_counter = d_counter;
   a.error_flag = d_counter + 1;
+  a.status = nullptr;
+  a.wait_ns = wait_ns_of(t);
+  a.skip_table_copy = t.test_skip_table_copy;
   a.G.mc2 = species->mass;
   a.G.mc2sq = species->mass * species->mass;
   a.G.p0c = p0c;
   a.G.mal = species->max_aperture_limit;
   a.G.ap_on = species->aperture_limit_on;
   a.G.charge = species->charge;
-  const int block = t.threads_per_block;
-  size_t smem = (size_t)a.table_dw * 8 + (t.compact_every > 0 ? (size_t)9 * block * 8 : 0) +
-                (size_t)bgt::QMEMO_CLASSES * 13 * block * 8;
-  if (smem > 200 * 1024) return fail(BGT_ETOOLARGE, "element table does not fit in shared memory");
   const int64_t n_tiles = (n + block - 1) / block;
   int64_t grid = std::min<int64_t>((int64_t)sms * t.blocks_per_sm, n_tiles);
   if (grid < 1) grid = 1;
-  // the counter and error flag must start at zero for every launch
+  // the counter and error flag must start at zero for every call
   if ((ce = cudaMemsetAsync(d_counter, 0, 2 * sizeof(int32_t), st)) != cudaSuccess)
     return fail(BGT_ECUDA, std::string("scratch clear: ") + cudaGetErrorString(ce));
   const int32_t seg = t.turns_per_launch > 0 ? t.turns_per_launch : n_turns;
@@ -848,10 +1102,12 @@ extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n
     a.n_turns = std::min(seg, n_turns - k);
     if (k > 0 && (ce = cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st)) != cudaSuccess)
       return fail(BGT_ECUDA, std::string("scratch clear: ") + cudaGetErrorString(ce));
-    if (!((block == 128 && t.blocks_per_sm == 4) || (block == 256 && t.blocks_per_sm == 2)))
-      return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: tuning must be (128, 4) or (256, 2)");
-    ce = find_track_kernel(block, t.blocks_per_sm, 0, rare)(a, (int)grid, smem, st);
+    ce = launch(a, (int)grid, smem, st);
     if (ce != cudaSuccess) return fail(BGT_ECUDA, std::string("track_kernel launch: ") + cudaGetErrorString(ce));
   }
+  // the call's error flag (1 = a table-staging wait ran out) for the caller
+  if (d_status &&
+      (ce = cudaMemcpyAsync(d_status, d_counter + 1, sizeof(int32_t), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+    return fail(BGT_ECUDA, std::string("status copy: ") + cudaGetErrorString(ce));
   return 0;
 }

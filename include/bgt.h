@@ -37,9 +37,24 @@
  *    which the particle was lost (bunch%ix_turn before that turn,
  *    lt_tracking_mod.f90:1633).  Both stay -1 for particles that survive.
  *  - Every function returns 0 on success or a negative BGT_E* code; the
- *    message is available from bgt_last_error().  Nothing aborts.
+ *    message is available from bgt_last_error() on the same thread.
+ *    Nothing aborts.
  *  - Host buffers are caller-owned; device buffers are owned by the handle or
  *    by the caller (the *_device entry points).
+ *
+ * Threading.  The reference calls track1 from OpenMP threads
+ * (bmad/multiparticle/beam_utils.f90:69-74) and track_many from the parallel
+ * sections of its DA scan (bmad/modules/dynamic_aperture_mod.f90:163-196).
+ * Every entry point that takes a handle is re-entrant: any number of threads
+ * may call it on one handle at the same time.  Each call takes a context of
+ * its own from the handle's pool -- a library-owned stream, staging buffers
+ * and the kernel's tile counter and error flag -- so concurrent calls never
+ * share buffers; the host-buffer calls wait for their own stream only (no
+ * device-wide synchronisation).  Device-buffer calls run on the caller's
+ * stream, ordered after the previous GPU work of the context they use, and
+ * are serialised per stream as CUDA orders them.  bgt_set_tuning takes
+ * effect for calls that start after it returns.  bgt_destroy must not run
+ * concurrently with other calls on the same handle.
  *
  * Scope: forward tracking (direction = time_dir = orientation = +1), relative
  * RF time (bmad_com%absolute_time_tracking = F), magnetic and electric
@@ -158,6 +173,13 @@ typedef struct bgt_tuning {
                                 from global memory; 1 = shared memory only; 2 = global memory;
                                 3 = global memory with every warp scheduled on its own (no
                                 CTA-wide tiles: for small, long-lived particle sets) */
+  int32_t wait_limit_us;     /* bound of the kernel's wait for its element-table copy, in
+                                microseconds (0 = 2 s); when it runs out the kernel sets its error
+                                flag and returns: BGT_ETIMEOUT from host-buffer calls, from
+                                bgt_device_status for device-buffer calls */
+  int32_t test_skip_table_copy; /* tests only: 1 = arm the table copy's barrier but issue no copy,
+                                   so every staging wait runs out (exercises the bounded wait and
+                                   the error path); 0 in normal use */
 } bgt_tuning;
 
 typedef struct bgt_handle bgt_handle;
@@ -190,7 +212,8 @@ int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, i
 
 /*
  * Same, DEVICE buffers already resident in HBM, enqueued on `stream`
- * (a cudaStream_t, NULL = legacy default stream).  Asynchronous.
+ * (a cudaStream_t, NULL = legacy default stream).  Asynchronous: a staging
+ * timeout on the device is reported by bgt_device_status.
  * Uses library-owned scratch sized on first use (grown as needed).
  * d_variant (device int32[n], may be NULL = variant 0) must be sorted
  * (non-decreasing); with it and more than one variant the call counts the
@@ -200,6 +223,15 @@ int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, i
 int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state,
                            int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n,
                            int32_t turn0, int32_t n_turns, void* stream);
+
+/*
+ * Waits for `stream` and reports whether any device-buffer call on this
+ * handle hit a table-staging timeout on the device since the last check
+ * (BGT_ETIMEOUT), clearing the flag; 0 otherwise.  The device-side
+ * counterpart of the err_flag the reference's tracking routines return
+ * (track1.f90:38-40 keeps particle loss a state, not an error).
+ */
+int bgt_device_status(bgt_handle* h, void* stream);
 
 /*
  * Track n particles through table elements [e_begin, e_end) of their variant
@@ -217,17 +249,17 @@ int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, int32_t* state
  * orbit of variant v at the d-th momentum offset: its closed orbit with pz
  * set to that offset, plus eta*pz when the caller includes it, as
  * dynamic_aperture_mod.f90:132-140 forms it -- plus (r cos a, 0,
- * r sin a * y_scale, 0, 0, 0), and is tracked n_turns turns.  The offsets
- * themselves are part of ref_orbit: deltas[] (n_delta values, may be NULL)
- * is not read.  da_radius[((v * n_delta) + d) * n_angle + a] receives
+ * r sin a * y_scale, 0, 0, 0), and is tracked n_turns turns.  The
+ * momentum offsets are part of ref_orbit (its pz entries).
+ * da_radius[((v * n_delta) + d) * n_angle + a] receives
  * the largest grid radius below the first lost one along that ray (the
  * lower bracket x0 of dynamic_aperture_point, dynamic_aperture_mod.f90:
  * 335-388); survive_turns (optional, may be NULL) receives, per particle in
  * (v, d, a, r) order, the turns survived (n_turns if never lost).
  */
-int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_used, const double* deltas,
-                     int32_t n_delta, int32_t n_angle, double angle_min, double angle_max, int32_t n_radius,
-                     double r_max, double y_scale, int32_t n_turns, double* da_radius, int32_t* survive_turns);
+int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_used, int32_t n_delta,
+                     int32_t n_angle, double angle_min, double angle_max, int32_t n_radius, double r_max,
+                     double y_scale, int32_t n_turns, double* da_radius, int32_t* survive_turns);
 
 /* Number of this library's kernels launched since the handle was created. */
 int64_t bgt_kernel_launch_count(const bgt_handle* h);
@@ -244,19 +276,24 @@ int64_t bgt_kernel_launch_count(const bgt_handle* h);
  *
  * Limits: the array holds 256 KiB (table plus a 256-byte header) on every
  * GPU that loads the library, until the process exits; larger tables are
- * rejected with BGT_ETOOLARGE.  Every call reuses the same array and leaves
- * its contents behind, so calls that overlap on the GPU (other streams or
- * threads) race: serialise them.  The first call on a device looks up the
- * array's address and uploads constant tables; make it before any stream
- * capture.  tuning may be NULL; otherwise (threads, CTAs per SM) must be
- * (128, 4) or (256, 2) (table_mode is ignored: the table is always staged in
- * shared memory).  On error a message is written to err (err_len bytes).
+ * rejected with BGT_ETOOLARGE.  A table that fits the array but not the
+ * kernel's shared memory is read in place from the array.  Every call
+ * reuses the same array and leaves its contents behind, so calls that
+ * overlap on the GPU (other streams or threads) race: serialise them.  The
+ * first call on a device looks up the array's address and uploads constant
+ * tables; make it before any stream capture.  tuning may be NULL; otherwise
+ * (threads, CTAs per SM) must be (128, 4) or (256, 2), checked before
+ * anything is enqueued (table_mode is ignored).  d_status (device int32, may
+ * be NULL) receives, in stream order, the call's error flag: 1 when a
+ * table-staging wait on the device ran out, else 0.  The caller's current
+ * device is left as it was.  On error a message is written to err (err_len
+ * bytes).
  */
 int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n_ele, const bgt_species* species,
                                    double* d_vec6, double* d_beta, int32_t* d_state, int32_t* d_ix_ele_lost,
                                    int32_t* d_ix_turn_lost, int64_t n, int32_t turn0, int32_t n_turns,
-                                   const bgt_tuning* tuning, int32_t device, void* stream, char* err,
-                                   int32_t err_len);
+                                   const bgt_tuning* tuning, int32_t device, void* stream, int32_t* d_status,
+                                   char* err, int32_t err_len);
 
 /* Measured FP64 FMA throughput of `device` in TFLOP/s (2 flops per FMA):
  * the roofline denominator for the tracking kernel.  No reference

@@ -138,6 +138,16 @@ int dmh_track(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const 
   return 0;
 }
 
+// Bytes of one variant's compiled table (what bgt_table_info reports), or a
+// negative code when an element is rejected.
+int64_t dmh_table_bytes(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const bgt_species* sp) {
+  Tables T;
+  std::string msg;
+  int rc = host::compile_tables(eles, n_ele, n_variants, *sp, QMEMO_CLASSES, T.all, T.off, T.table_dw, T.rare,
+                                msg);
+  return rc ? rc : (int64_t)T.table_dw * 8;
+}
+
 // Whether the compiled tables need the RARE kernel instance (1), do not (0),
 // or a negative code when an element is rejected.
 int dmh_needs_rare(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const bgt_species* sp) {

@@ -1,8 +1,8 @@
 """Extract the reference's golden vectors for the bmad_standard path into
-tests/golden/*.json.  Reads the reference checkout (default /root/reference)
+tests/golden/*.json.  Reads the reference checkout given on the command line
 as text; the JSON files are committed so tests never need the reference.
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 Sources (relative to the reference root):
   regression_tests/tracking_method_test/output.correct  ("<ELE>: Bmad_Standard" rows)
@@ -72,4 +72,6 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+    main(Path(sys.argv[1]))

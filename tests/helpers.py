@@ -255,3 +255,49 @@ def oracle_da_survival(lattices, ref, n_angle, angle_min, angle_max, n_radius, r
         surv = np.where(st == 1, n_turns, it)
         out[v] = surv.reshape(nd, n_angle, n_radius)
     return out
+
+
+def result_digest(vec6, beta, state, ix_ele_lost, ix_turn_lost) -> str:
+    """SHA-256 of a tracking result's bytes (coordinates, beta, state, loss
+    element, loss turn): equal digests mean bit-identical results."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for a, dt in ((vec6, np.float64), (beta, np.float64), (state, np.int32), (ix_ele_lost, np.int32),
+                  (ix_turn_lost, np.int32)):
+        h.update(np.ascontiguousarray(a, dtype=dt).tobytes())
+    return h.hexdigest()
+
+
+def plain_rel_err(g: np.ndarray, o: np.ndarray) -> np.ndarray:
+    """Per particle, the largest plain per-coordinate relative error
+    max_c |g_c - o_c| / |o_c| (0 where the values are equal, inf where o_c is
+    0 and g_c is not): the north_star's "relative per coordinate" with no
+    floor, so a coordinate passing near zero counts at its own size."""
+    d = np.abs(np.asarray(g, np.float64) - np.asarray(o, np.float64))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(d == 0, 0.0, d / np.abs(o))
+    return np.max(r, axis=0)
+
+
+def exceed_digest(idx: np.ndarray) -> str:
+    """SHA-256 of a sorted index list (the particles above a bound)."""
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(np.sort(idx), dtype=np.int64).tobytes()).hexdigest()
+
+
+# Full-size parity cases: the configuration's ring and beam at its own size.
+# (name, lattice factory kwargs, beam spec name, particles, turns)
+CONFIG_PARITY_CASES = {
+    "config0": dict(apertures=False, beam="CONFIG0_BEAM", n=10_000, turns=1000),
+    "config1": dict(apertures=True, beam="CONFIG1_BEAM", n=20_000, turns=1000),
+}
+
+
+def config_parity_inputs(name: str):
+    """(lattice, vec6) of a full-size parity case."""
+    c = CONFIG_PARITY_CASES[name]
+    lat = rings.fodo_ring(apertures=c["apertures"])
+    v0 = rings.gaussian_beam(getattr(rings, c["beam"]), n=c["n"])
+    return lat, v0

@@ -33,7 +33,7 @@ def test_struct_layout_matches_header():
     # bgt_element: 12 int32 + 35 doubles + 6 x 22 doubles + 4 doubles
     assert ctypes.sizeof(_lib.BgtElement) == 12 * 4 + 35 * 8 + 6 * 22 * 8 + 4 * 8 + 8 * 8
     assert ctypes.sizeof(_lib.BgtSpecies) == 24
-    assert ctypes.sizeof(_lib.BgtTuning) == 20
+    assert ctypes.sizeof(_lib.BgtTuning) == 28
 
 
 def test_struct_offsets_match_the_c_compiler(tmp_path):

@@ -1,0 +1,91 @@
+"""GPU parity at the configurations' own sizes: the config-0 ring and beam
+(10,000 particles, 1000 turns, no apertures) and the config-1 ring with its
+apertures and beam (20,000 of its particles, 1000 turns).
+
+* Against the correctly rounded oracle build: bit-identical.  After one turn
+  the oracle runs here; after 1000 turns its result is the SHA-256 digest
+  tests/golden/make_config_parity.py recorded (that build is ~7x slower than
+  the glibc one, minutes at these sizes).
+* Against the glibc oracle build (the reference's arithmetic), run here:
+  states, loss elements and loss turns exact; coordinates within
+  north_star's bounds -- 1e-13 after one turn, 1e-9 after 1000 turns,
+  relative per coordinate -- for every particle except those on which the
+  two CPU builds of the oracle already differ by more than the bound (glibc
+  not correctly rounded on a fraction of asin/sin/atan2 arguments, amplified
+  by the exact bend).  The test shows those are exactly the same particles,
+  and prints the counts.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from bgt import lattice as L
+from bgt.track import Tracker
+
+from helpers import (CONFIG_PARITY_CASES, config_parity_inputs, exceed_digest, oracle_track_elements, plain_rel_err,
+                     result_digest)
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_PATH = Path(__file__).resolve().parent / "golden" / "config_parity.json"
+
+
+def _golden():
+    return json.loads(GOLDEN_PATH.read_text())
+
+
+def _gpu(lat, v0, turns):
+    tr = Tracker(lat)
+    b = tr.make_bunch(v0.copy())
+    tr.track_turns(b, turns)
+    return b
+
+
+@pytest.mark.parametrize("name", sorted(CONFIG_PARITY_CASES))
+def test_full_size_one_turn(name):
+    lat, v0 = config_parity_inputs(name)
+    b = _gpu(lat, v0, 1)
+    cr = oracle_track_elements(lat, v0, 0, len(lat), 1, variant="cr")
+    assert np.array_equal(b.vec6, cr[0]) and np.array_equal(b.beta, cr[1])
+    assert np.array_equal(b.state, cr[2]) and np.array_equal(b.ix_ele_lost, cr[3])
+    assert result_digest(b.vec6, b.beta, b.state, b.ix_ele_lost, b.ix_turn_lost) == _golden()[name]["1"]["digest_cr"]
+    gl = oracle_track_elements(lat, v0, 0, len(lat), 1, variant="glibc")
+    _compare_glibc(name, 1, b, cr, gl)
+
+
+@pytest.mark.parametrize("name", sorted(CONFIG_PARITY_CASES))
+def test_full_size_1000_turns(name):
+    c = CONFIG_PARITY_CASES[name]
+    lat, v0 = config_parity_inputs(name)
+    b = _gpu(lat, v0, c["turns"])
+    # bit-identical to the correctly rounded oracle (recorded digest)
+    g = _golden()[name][str(c["turns"])]
+    assert result_digest(b.vec6, b.beta, b.state, b.ix_ele_lost, b.ix_turn_lost) == g["digest_cr"]
+    assert int(np.sum(b.state != L.ALIVE)) == g["lost_cr"]
+    gl = oracle_track_elements(lat, v0, 0, len(lat), c["turns"], variant="glibc")
+    _compare_glibc(name, c["turns"], b, None, gl)
+
+
+def _compare_glibc(name, turns, b, cr, gl):
+    g = _golden()[name][str(turns)]
+    # loss state, element and turn exact for every particle
+    assert np.array_equal(b.state, gl[2])
+    assert np.array_equal(b.ix_ele_lost, gl[3])
+    assert np.array_equal(b.ix_turn_lost, gl[4])
+    alive = (b.state == L.ALIVE) & (gl[2] == L.ALIVE)
+    err = plain_rel_err(b.vec6, gl[0])
+    idx = np.nonzero(alive & (err > g["bound"]))[0]
+    # the same particles as between the two CPU builds of the oracle
+    assert idx.size == g["exceed_count"]
+    assert exceed_digest(idx) == g["exceed_digest"]
+    if cr is not None:
+        idx_cpu = np.nonzero(alive & (plain_rel_err(cr[0], gl[0]) > g["bound"]))[0]
+        assert np.array_equal(idx, idx_cpu)
+    within = alive.sum() - idx.size
+    print(f"\nPARITY {name} turns={turns} particles={b.n} alive={int(alive.sum())} "
+          f"within {g['bound']:.0e} of glibc: {int(within)} ({100.0 * within / max(1, alive.sum()):.2f}%), "
+          f"above: {idx.size} (same particles as CR-oracle vs glibc-oracle), "
+          f"max plain rel err {float(np.max(err[alive])) if alive.any() else 0.0:.2e}, "
+          f"lost {int(np.sum(b.state != L.ALIVE))} (state/element/turn exact)")

@@ -128,7 +128,31 @@ def test_null_handle_calls_return_einval():
     assert lib.bgt_table_info(None, None, None) == _lib.BGT_EINVAL
     assert lib.bgt_kernel_launch_count(None) == -1
     assert lib.bgt_last_error(None) == b"null handle"
+    assert lib.bgt_device_status(None, None) == _lib.BGT_EINVAL
+    assert lib.bgt_da_scan_grid(None, dp, 1, 1, 4, 0.0, 1.0, 8, 0.01, 1.0, 10, dp, None) == _lib.BGT_EINVAL
     assert lib.bgt_destroy(None) == 0
+
+
+def test_error_messages_are_per_thread():
+    """bgt_last_error returns the message of the last failed call on the
+    calling thread: a failure on another thread does not replace it."""
+    import threading
+
+    lib = _lib.load()
+    t = _lib.BgtTuning(128, 4, 0, 0, 0)
+    assert lib.bgt_get_tuning(None, C.byref(t)) == _lib.BGT_EINVAL
+    mine = lib.bgt_last_error(None)
+    other = []
+
+    def worker():
+        lib.bgt_track_elements(None, None, None, None, None, None, 1, 0, 1)
+        other.append(lib.bgt_last_error(None))
+
+    th = threading.Thread(target=worker)
+    th.start()
+    th.join()
+    assert other and other[0] != mine
+    assert lib.bgt_last_error(None) == mine
 
 
 def test_noalloc_checks_arguments_first():
@@ -139,5 +163,14 @@ def test_noalloc_checks_arguments_first():
     buf = C.create_string_buffer(256)
     # no particle buffers: rejected before any device call
     rc = lib.bgt_track_turns_device_noalloc(arr, n_ele, C.byref(sp), None, None, None, None, None, 10, 0, 1,
-                                             None, 0, None, buf, 256)
+                                             None, 0, None, None, buf, 256)
     assert rc == _lib.BGT_EINVAL and b"invalid argument" in buf.value
+    # a launch shape without a kernel instance, or a bad tuning value, is
+    # refused before any device call (the pointers below are never read)
+    fake = C.c_void_p(16)
+    for tun, what in ((_lib.BgtTuning(64, 8, 0, 0, 0), b"tuning must be"),
+                      (_lib.BgtTuning(128, 4, 0, -1, 0), b"invalid tuning"),
+                      (_lib.BgtTuning(256, 2, 0, 0, 0, 0, 2), b"invalid tuning")):
+        rc = lib.bgt_track_turns_device_noalloc(arr, n_ele, C.byref(sp), fake, fake, fake, fake, None, 10, 0, 1,
+                                                 C.byref(tun), 0, None, None, buf, 256)
+        assert rc == _lib.BGT_EINVAL and what in buf.value, buf.value
