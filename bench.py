@@ -36,7 +36,7 @@ UNIT = "particle*turns/s"
 N_PARTICLES = 1_000_000
 # FP64 operations per particle.turn on this ring (add/sub/mul/div/sqrt = 1
 # each) and libm calls per particle.turn, counted by the instrumented oracle
-# build over the config-1 beam (tests/test_flop_count.py keeps these current).
+# build over the config-1 beam (tests/test_flop_count.py pins them to that count).
 FLOPS_PER_PARTICLE_TURN = 98807.0
 LIBM_PER_PARTICLE_TURN = 2315.0
 
@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--jitter", action="store_true", help="learned-da: add one jittered probe per grid cell")
     ap.add_argument("--boundary-cells", default="", help="pruned scans: grid cells either side of the predicted "
                     "DA boundary tracked in full; comma list (learned-da default 0,2; sext-scan 2)")
+    ap.add_argument("--p-lo", default="", help="pruned scans: retire probes with p(lost) < p_lo as surviving; 0 "
+                    "(default) follows the method's rule (only confidently lost probes retired early); a comma "
+                    "list (e.g. 0,0.02) adds measured comparisons outside the rule")
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--model", default="", help="sext-scan: start from this saved classifier (fine-tune)")
@@ -198,11 +201,69 @@ def cpu_baseline():
 
 
 # ---------------------------------------------------------------------------
-# Dynamic-aperture workloads (one GPU): the batched scan of error variants,
-# the classifier-pruned scan against the plain one, and the pruned
-# sextupole-setting scan.  Each prints one JSON line.
+# Dynamic-aperture workloads: the batched scan of error variants, the
+# classifier-pruned scan against the plain one, and the pruned
+# sextupole-setting scan.  Each prints one JSON line (rank 0).  Under
+# torchrun the variants are sharded over ranks (bgt.da.sharded_scan: one
+# contiguous block of variants per GPU, DA radii all-gathered, wall time the
+# max over ranks); the classifier's training samples are all-gathered so that
+# every rank trains the same network (bgt.learned_da.gather_rows).
 
-def _da_problem(lats, grid, turns):
+class Ranks:
+    """rank / world / device of this process, and the reductions the DA
+    workloads need (NCCL under torchrun; identity on one GPU)."""
+
+    def __init__(self):
+        import torch
+
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        self.dev = torch.device("cuda", self.local)
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def _red(self, x, op):
+        if not self.dist:
+            return x
+        import torch
+
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def sum(self, x):
+        return self._red(x, self.dist.ReduceOp.SUM if self.dist else None)
+
+    def max(self, x):
+        return self._red(x, self.dist.ReduceOp.MAX if self.dist else None)
+
+    def all(self, flag: bool) -> bool:
+        return self._red(1.0 if flag else 0.0, self.dist.ReduceOp.MIN if self.dist else None) > 0.5
+
+    def gather_rows(self, t):
+        from bgt import learned_da as LD
+
+        return LD.gather_rows(t) if self.dist else t
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def _da_problem(lats, grid, turns, device=0):
     import dataclasses
 
     from bgt import da, rings
@@ -211,7 +272,7 @@ def _da_problem(lats, grid, turns):
 
     g = dataclasses.replace(grid, n_turns=turns)
     ys = da.y_scale(rings.TWISS0["beta_a"], rings.TWISS0["beta_b"])
-    return LD.setup(Tracker(lats), lats, g, (rings.K2_SF, rings.K2_SD), yscale=ys)
+    return LD.setup(Tracker(lats, device=device), lats, g, (rings.K2_SF, rings.K2_SD), yscale=ys)
 
 
 def _autotune_da(pb, turns=2, fixed=""):
@@ -264,43 +325,62 @@ def da_cpu_baseline(lat, pb, n_probe=512, turns=20):
 
 
 def run_da(args):
-    """Batched DA scan: every probe of every error variant in one launch."""
+    """Batched DA scan: every probe of every error variant in one launch (per
+    GPU: its block of variants in one launch)."""
     import torch
 
     from bgt import da, rings
 
+    R = Ranks()
     nv = args.variants or 256
+    if nv < R.world:
+        raise SystemExit("more GPUs than variants")
     turns = args.da_turns or rings.CONFIG2_GRID.n_turns
     t0 = time.perf_counter()
     lats = rings.error_variants(nv)
-    pb = _da_problem(lats, rings.CONFIG2_GRID, turns)
-    t_setup = time.perf_counter() - t0
-    tun = _autotune_da(pb, fixed=args.tuning)
-    launches0 = pb.tracker.launch_count
-    with ClockSampler(torch.cuda.current_device()) as clk:
+    info = {}
+
+    def scan(b, e):
+        pb = _da_problem(lats[b:e], rings.CONFIG2_GRID, turns, R.local)
+        info["setup_s"] = time.perf_counter() - t0
+        info["tuning"] = _autotune_da(pb, fixed=args.tuning)
+        info["pb"] = pb
+        launches0 = pb.tracker.launch_count
+        R.barrier()
         res = da.plain_scan(pb.tracker, pb.ref, **pb.grid())
-    n = nv * pb.per_variant
-    line = {"metric": "DA scan wall time, error variants x polar grid (one launch)", "value": res.wall_s,
-            "unit": "s", "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched DA scan of error variants", "variants": nv, "probes": n,
-                       "probes_per_variant": pb.per_variant, "turns": turns, "angles": pb.n_angle,
-                       "radii": pb.n_radius, "r_max_m": pb.r_max, "deltas": list(pb.deltas)},
-            "particle_turns": res.particle_turns, "particle_turns_per_s": res.particle_turns / res.wall_s,
-            "da_radius_mm_mean": _mm(res.radius),
-            "da_radius_mm_mean_per_delta": [_mm(res.radius[:, d]) for d in range(len(pb.deltas))],
-            "setup_s": t_setup, "tuning": tun, "gpu_launches": pb.tracker.launch_count - launches0,
-            "clocks": clk.summary()}
-    if not args.no_cpu_baseline:
-        cpu = da_cpu_baseline(lats[0], pb)
-        line["cpu_baseline"] = cpu
-        line["cpu_estimate_s"] = res.particle_turns / cpu["value"]
-    print(json.dumps(line), flush=True)
+        info["launches"] = pb.tracker.launch_count - launches0
+        return res
+
+    with ClockSampler(R.local) as clk:
+        sh = da.sharded_scan(scan, nv, R.rank, R.world)
+    pb = info["pb"]
+    if R.rank == 0:
+        n = nv * pb.per_variant
+        line = {"metric": "DA scan wall time, error variants x polar grid (one launch per GPU)",
+                "value": sh.wall_s, "unit": "s", "higher_is_better": False, "n_gpus": R.world,
+                "scaling": "strong", "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "batched DA scan of error variants", "variants": nv, "probes": n,
+                           "probes_per_variant": pb.per_variant, "turns": turns, "angles": pb.n_angle,
+                           "radii": pb.n_radius, "r_max_m": pb.r_max, "deltas": list(pb.deltas),
+                           "parallelism": f"variants x{R.world} GPUs"},
+                "particle_turns": sh.particle_turns, "particle_turns_per_s": sh.particle_turns / sh.wall_s,
+                "da_radius_mm_mean": _mm(sh.radius),
+                "da_radius_mm_mean_per_delta": [_mm(sh.radius[:, d]) for d in range(len(pb.deltas))],
+                "setup_s": info["setup_s"], "tuning": info["tuning"], "gpu_launches": info["launches"],
+                "clocks": clk.summary()}
+        if not args.no_cpu_baseline and R.world == 1:
+            cpu = da_cpu_baseline(lats[0], pb)
+            line["cpu_baseline"] = cpu
+            line["cpu_estimate_s"] = sh.particle_turns / cpu["value"]
+        print(json.dumps(line), flush=True)
+    R.close()
 
 
-def _train_classifier(args, pb, scans, net, fine_tune=False):
+def _train_classifier(args, R, pb, scans, net, fine_tune=False):
     from bgt import learned_da as LD
 
     raw, lab = LD.training_set(pb, scans, net)
+    raw, lab = R.gather_rows(raw), R.gather_rows(lab)
     hist, t_train = LD.train(net, raw, lab, epochs=args.epochs if not fine_tune else max(2, args.epochs // 2),
                              batch=8192, lr=2e-3 if not fine_tune else 1e-3, seed=args.seed,
                              set_normalization=not fine_tune)
@@ -313,74 +393,106 @@ def _train_classifier(args, pb, scans, net, fine_tune=False):
             "gemm_tflops": flops / t_train / 1e12}
 
 
+def _staged_scan_sharded(R, lats, grid, turns, n, jitter_seeds=(None,), tun=None):
+    """Staged plain scans (turn-64 snapshot) of this rank's block of the
+    variants lats[:n]: (ScanProblem, [StagedScan], wall max over ranks)."""
+    from bgt import da
+    from bgt import learned_da as LD
+
+    b, e = da.shard_range(n, R.rank, R.world)
+    pb = _da_problem(lats[b:e], grid, turns, R.local)
+    if tun:
+        pb.tracker.set_tuning(**tun)
+    R.barrier()
+    scans = [LD.staged_scan(pb, 0, e - b, jitter_seed=j) for j in jitter_seeds]
+    return pb, scans, R.max(sum(s.wall_s for s in scans))
+
+
 def run_learned_da(args):
     """Classifier-pruned DA scan vs the plain scan on held-out variants."""
-    import torch
-
     from bgt import da, rings
     from bgt import learned_da as LD
     from bgt.mlp import SurvivalMLP
 
+    R = Ranks()
     nv = args.variants or 256
     turns = args.da_turns or rings.CONFIG2_GRID.n_turns
     half = nv // 2
+    if half < R.world:
+        raise SystemExit("more GPUs than held-out variants")
     lats = rings.error_variants(nv)
-    pb_tr = _da_problem(lats[:half], rings.CONFIG2_GRID, turns)
-    pb_te = _da_problem(lats[half:], rings.CONFIG2_GRID, turns)
+    held = lats[half:]
+    bh, eh = da.shard_range(nv - half, R.rank, R.world)
+    pb_te = _da_problem(held[bh:eh], rings.CONFIG2_GRID, turns, R.local)
     tun = _autotune_da(pb_te, fixed=args.tuning)
-    pb_tr.tracker.set_tuning(**tun)
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        scans = [LD.staged_scan(pb_tr, 0, half)]
-        if args.jitter:
-            scans.append(LD.staged_scan(pb_tr, 0, half, jitter_seed=args.seed))
+    p_los = [float(x) for x in (args.p_lo or "0").split(",")]
+    bcs = [int(c) for c in (args.boundary_cells or "0,2").split(",")]
+    with ClockSampler(R.local) as clk:
+        jit = (None, args.seed) if args.jitter else (None,)
+        pb_tr, scans, train_scan_s = _staged_scan_sharded(R, lats, rings.CONFIG2_GRID, turns, half, jit, tun)
         net = SurvivalMLP(max_batch=16384, seed=args.seed)
-        train = _train_classifier(args, pb_tr, scans, net)
-        plain = da.plain_scan(pb_te.tracker, pb_te.ref, **pb_te.grid())
-        bcs = [int(c) for c in (args.boundary_cells or "0,2").split(",")]
-        prs = [LD.pruned_scan(pb_te, net, 0, nv - half, seed=args.seed, boundary_cells=c) for c in bcs]
-    if args.save_model:
+        train = _train_classifier(args, R, pb_tr, scans, net)
+        R.barrier()
+        plain = da.sharded_scan(lambda b, e: da.plain_scan(pb_te.tracker, pb_te.ref, **pb_te.grid()), nv - half,
+                                R.rank, R.world)
+        runs = []
+        for pl in p_los:
+            for c in bcs:
+                R.barrier()
+                pr = da.sharded_scan(lambda b, e: LD.pruned_scan(pb_te, net, 0, e - b, seed=args.seed + R.rank,
+                                                                 boundary_cells=c, p_lo=pl),
+                                     nv - half, R.rank, R.world)
+                runs.append((pl, c, pr))
+    if args.save_model and R.rank == 0:
         net.save(args.save_model)
-    plain_surv = (plain.survive_turns >= turns).reshape(-1)
+    plain_surv = (plain.local.survive_turns >= turns).reshape(-1)
     dr = pb_te.r_max / (pb_te.n_radius - 1)
 
-    def summary(pr, c):
-        cells = np.abs(pr.radius - plain.radius) / dr
-        return {"boundary_cells": c, "speedup": plain.wall_s / pr.wall_s, "pruned_s": pr.wall_s,
-                "da_error": da.da_error(pr.radius, plain.radius), "rays_exact_fraction": float(np.mean(cells < 0.5)),
-                "max_error_cells": float(np.max(cells)), "pruned_particle_turns": pr.particle_turns,
-                "tracked_fraction": pr.n_tracked / pr.n_probes, "retired_lost": pr.n_retired_lost,
-                "retired_survive": pr.n_retired_survive, "audit_probes": pr.audit_n,
-                "audit_errors": pr.audit_errors,
-                "tracked_outcomes_equal_plain": bool(np.array_equal(pr.survive_label[pr.tracked],
-                                                                    plain_surv[pr.tracked])),
-                "da_radius_mm_mean": _mm(pr.radius)}
+    def summary(pl, c, sh):
+        pr = sh.local
+        cells = np.abs(sh.radius - plain.radius) / dr
+        return {"p_lo": pl, "boundary_cells": c,
+                "rule": "north_star: only confidently lost probes retired early" if pl == 0 else
+                        "retires confident survivors too (outside north_star's rule; comparison only)",
+                "speedup": plain.wall_s / sh.wall_s, "pruned_s": sh.wall_s,
+                "da_error": da.da_error(sh.radius, plain.radius), "rays_exact_fraction": float(np.mean(cells < 0.5)),
+                "max_error_cells": float(np.max(cells)), "pruned_particle_turns": sh.particle_turns,
+                "particle_turns_ratio": plain.particle_turns / max(1, sh.particle_turns),
+                "tracked_fraction": R.sum(pr.n_tracked) / R.sum(pr.n_probes),
+                "retired_lost": int(R.sum(pr.n_retired_lost)), "retired_survive": int(R.sum(pr.n_retired_survive)),
+                "audit_probes": int(R.sum(pr.audit_n)), "audit_errors": int(R.sum(pr.audit_errors)),
+                "tracked_outcomes_equal_plain": R.all(bool(np.array_equal(pr.survive_label[pr.tracked],
+                                                                           plain_surv[pr.tracked]))),
+                "da_radius_mm_mean": _mm(sh.radius)}
 
-    runs = [summary(pr, c) for pr, c in zip(prs, bcs)]
-    # the headline: the fastest setting whose DA error is within 2 %
-    ok = [r for r in runs if r["da_error"] <= 0.02] or runs
+    runs = [summary(pl, c, sh) for pl, c, sh in runs]
+    # the headline: the fastest rule-following setting whose DA error is within 2 %
+    rule = [r for r in runs if r["p_lo"] == 0] or runs
+    ok = [r for r in rule if r["da_error"] <= 0.02] or rule
     best = max(ok, key=lambda r: r["speedup"])
-    train_plain_s = scans[0].wall_s
-    line = {"metric": "DA-scan wall time, plain / classifier-pruned, held-out variants",
-            "value": best["speedup"], "unit": "x", "higher_is_better": True, "n_gpus": 1,
-            "dtype": "f64 tracking, bf16/fp32 classifier", "data": "synthetic",
-            "config": {"workload": "learned DA scan of error variants", "variants_train": half,
-                       "variants_heldout": nv - half, "probes_per_variant": pb_te.per_variant, "turns": turns,
-                       "early_turns": 64, "p_hi": 0.98, "p_lo": 0.02, "audit": 0.02,
-                       "boundary_cells": best["boundary_cells"], "jitter": bool(args.jitter)},
-            "plain_s": plain.wall_s, "pruned_s": best["pruned_s"], "da_error": best["da_error"],
-            "plain_particle_turns": plain.particle_turns, "pruned": runs,
-            "all_variants_plain": {"wall_s": train_plain_s + plain.wall_s, "launches": "2 x 128 variants",
-                                   "particle_turns": scans[0].particle_turns + plain.particle_turns,
-                                   "da_radius_mm_mean": _mm(np.concatenate(
-                                       [LD.radius_of(pb_tr, (scans[0].survive >= turns).cpu().numpy(), half),
-                                        plain.radius]))},
-            "train_scan_s": sum(s.wall_s for s in scans), "train": train,
-            "da_radius_mm_mean_plain": _mm(plain.radius), "tuning": tun, "clocks": clk.summary()}
-    if not args.no_cpu_baseline:
-        cpu = da_cpu_baseline(lats[half], pb_te)
-        line["cpu_baseline"] = cpu
-        line["cpu_estimate_plain_s"] = plain.particle_turns / cpu["value"]
-    print(json.dumps(line), flush=True)
+    train_pt = R.sum(sum(s.particle_turns for s in scans[:1]))
+    if R.rank == 0:
+        line = {"metric": "DA-scan wall time, plain / classifier-pruned, held-out variants",
+                "value": best["speedup"], "unit": "x", "higher_is_better": True, "n_gpus": R.world,
+                "scaling": "strong", "dtype": "f64 tracking, bf16/fp32 classifier", "data": "synthetic",
+                "config": {"workload": "learned DA scan of error variants", "variants_train": half,
+                           "variants_heldout": nv - half, "probes_per_variant": pb_te.per_variant, "turns": turns,
+                           "early_turns": 64, "p_hi": 0.98, "p_lo": best["p_lo"], "audit": 0.02,
+                           "boundary_cells": best["boundary_cells"], "jitter": bool(args.jitter),
+                           "parallelism": f"variants x{R.world} GPUs"},
+                "plain_s": plain.wall_s, "pruned_s": best["pruned_s"], "da_error": best["da_error"],
+                "plain_particle_turns": plain.particle_turns, "pruned": runs,
+                "all_variants_plain": {"wall_s": train_scan_s + plain.wall_s,
+                                       "launches": "2 x 128 variants (training scan staged at turn 64)",
+                                       "particle_turns": int(train_pt) + plain.particle_turns},
+                "train_scan_s": train_scan_s, "train": train,
+                "da_radius_mm_mean_plain": _mm(plain.radius), "tuning": tun, "clocks": clk.summary()}
+        if not args.no_cpu_baseline and R.world == 1:
+            cpu = da_cpu_baseline(lats[half], pb_te)
+            line["cpu_baseline"] = cpu
+            line["cpu_estimate_plain_s"] = plain.particle_turns / cpu["value"]
+        print(json.dumps(line), flush=True)
+    R.close()
 
 
 def run_sext_scan(args):
@@ -388,58 +500,71 @@ def run_sext_scan(args):
     prune the rest with the boundary verified by the tracker, rank all
     variants by DA, and compare the ranking of 256 audited variants with a
     plain-tracking ranking of the same variants."""
-    import torch
-
     from bgt import da, rings
     from bgt import learned_da as LD
     from bgt.mlp import SurvivalMLP
 
+    R = Ranks()
     nv = args.variants or 4096
     turns = args.da_turns or rings.CONFIG4_GRID.n_turns
     first = min(256, nv // 4)
     t0 = time.perf_counter()
     lats = rings.sextupole_variants(nv)
-    pb_ft = _da_problem(lats[:first], rings.CONFIG4_GRID, turns)
-    pb_rest = _da_problem(lats[first:], rings.CONFIG4_GRID, turns)
+    rest = lats[first:]
     rng = np.random.default_rng(args.seed)
     n_audit = min(256, nv - first)
     audit_idx = np.sort(rng.choice(nv - first, n_audit, replace=False))
-    pb_aud = _da_problem([lats[first + i] for i in audit_idx], rings.CONFIG4_GRID, turns)
+    audited = [rest[i] for i in audit_idx]
+    br, er = da.shard_range(nv - first, R.rank, R.world)
+    ba, ea = da.shard_range(n_audit, R.rank, R.world)
+    pb_rest = _da_problem(rest[br:er], rings.CONFIG4_GRID, turns, R.local)
+    pb_aud = _da_problem(audited[ba:ea], rings.CONFIG4_GRID, turns, R.local)
     t_setup = time.perf_counter() - t0
     tun = _autotune_da(pb_rest, fixed=args.tuning)
-    pb_ft.tracker.set_tuning(**tun)
     pb_aud.tracker.set_tuning(**tun)
     net = SurvivalMLP(max_batch=16384, seed=args.seed)
     fine = bool(args.model)
     if fine:
         net.load(args.model)
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        ft = LD.staged_scan(pb_ft, 0, first)
-        train = _train_classifier(args, pb_ft, [ft], net, fine_tune=fine)
-        bc = int((args.boundary_cells or "2").split(",")[0])
-        pr = LD.pruned_scan(pb_rest, net, 0, nv - first, seed=args.seed, boundary_cells=bc)
-        plain = da.plain_scan(pb_aud.tracker, pb_aud.ref, **pb_aud.grid())
-    if args.save_model:
+    bc = int((args.boundary_cells or "2").split(",")[0])
+    pl = float((args.p_lo or "0").split(",")[0])
+    with ClockSampler(R.local) as clk:
+        pb_ft, fts, ft_s = _staged_scan_sharded(R, lats, rings.CONFIG4_GRID, turns, first, (None,), tun)
+        ft = fts[0]
+        train = _train_classifier(args, R, pb_ft, [ft], net, fine_tune=fine)
+        R.barrier()
+        pr = da.sharded_scan(lambda b, e: LD.pruned_scan(pb_rest, net, 0, e - b, seed=args.seed + R.rank,
+                                                         boundary_cells=bc, p_lo=pl), nv - first, R.rank, R.world)
+        R.barrier()
+        plain = da.sharded_scan(lambda b, e: da.plain_scan(pb_aud.tracker, pb_aud.ref, **pb_aud.grid()), n_audit,
+                                R.rank, R.world)
+    if args.save_model and R.rank == 0:
         net.save(args.save_model)
     ft_surv = (ft.survive >= turns).cpu().numpy()
-    da_ft = LD.radius_of(pb_ft, ft_surv, first).mean(axis=(1, 2))
+    da_ft_local = LD.radius_of(pb_ft, ft_surv, pb_ft.n_variants)
+    da_ft = da.sharded_radii(da_ft_local, first, R.rank, R.world) if R.dist else da_ft_local
+    da_ft = da_ft.mean(axis=(1, 2))
     da_rest = pr.radius.mean(axis=(1, 2))
     da_all = np.concatenate([da_ft, da_rest])
     order = np.argsort(-da_all, kind="stable")
     ranking = LD.ranking_mismatches(da_rest[audit_idx], plain.radius.mean(axis=(1, 2)))
-    line = {"metric": "sextupole scan: ranking mismatches of pruned vs plain DA, audited variants",
-            "value": ranking["discordant_pairs"], "unit": "discordant pairs", "higher_is_better": False,
-            "n_gpus": 1, "dtype": "f64 tracking, bf16/fp32 classifier", "data": "synthetic",
-            "config": {"workload": "pruned sextupole-setting scan", "variants": nv, "fine_tune_variants": first,
-                       "probes_per_variant": pb_rest.per_variant, "turns": turns, "audited_variants": n_audit,
-                       "boundary_cells": bc, "start_model": args.model or None},
-            "ranking": ranking, "da_error_audited": da.da_error(pr.radius[audit_idx], plain.radius),
-            "pruned_s": pr.wall_s, "fine_tune_scan_s": ft.wall_s, "audit_plain_s": plain.wall_s,
-            "audit_plain_s_per_variant": plain.wall_s / n_audit, "pruned_s_per_variant": pr.wall_s / (nv - first),
-            "tracked_fraction": pr.n_tracked / pr.n_probes, "train": train,
-            "top10_variants_by_da": [[int(i), _mm(da_all[i])] for i in order[:10]],
-            "setup_s": t_setup, "tuning": tun, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    if R.rank == 0:
+        line = {"metric": "sextupole scan: ranking mismatches of pruned vs plain DA, audited variants",
+                "value": ranking["discordant_pairs"], "unit": "discordant pairs", "higher_is_better": False,
+                "n_gpus": R.world, "scaling": "strong", "dtype": "f64 tracking, bf16/fp32 classifier",
+                "data": "synthetic",
+                "config": {"workload": "pruned sextupole-setting scan", "variants": nv, "fine_tune_variants": first,
+                           "probes_per_variant": pb_rest.per_variant, "turns": turns, "audited_variants": n_audit,
+                           "boundary_cells": bc, "p_lo": pl, "start_model": args.model or None,
+                           "parallelism": f"variants x{R.world} GPUs"},
+                "ranking": ranking, "da_error_audited": da.da_error(pr.radius[audit_idx], plain.radius),
+                "pruned_s": pr.wall_s, "fine_tune_scan_s": ft_s, "audit_plain_s": plain.wall_s,
+                "audit_plain_s_per_variant": plain.wall_s / n_audit, "pruned_s_per_variant": pr.wall_s / (nv - first),
+                "tracked_fraction": R.sum(pr.local.n_tracked) / R.sum(pr.local.n_probes), "train": train,
+                "top10_variants_by_da": [[int(i), _mm(da_all[i])] for i in order[:10]],
+                "setup_s": t_setup, "tuning": tun, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    R.close()
 
 
 def main():

@@ -259,3 +259,37 @@ def sharded_radii(local: np.ndarray, n_variants: int, rank: int, world: int, gro
     dist.all_gather(parts, t, group=group)
     full = np.concatenate([p.cpu().numpy() for p in parts], axis=0)
     return full[:n_variants]
+
+
+@dataclass
+class ShardedScan:
+    radius: np.ndarray  # [n_variants, d, a], all variants (gathered)
+    local: DAResult  # this rank's scan of its block
+    begin: int  # this rank's block of variants [begin, end)
+    end: int
+    wall_s: float  # max over ranks
+    particle_turns: int  # summed over ranks
+
+
+def sharded_scan(scan, n_variants: int, rank: int = 0, world: int = 1, group=None) -> ShardedScan:
+    """A DA scan sharded by lattice variant: `scan(v_begin, v_end)` -> DAResult
+    runs on this rank's contiguous block (shard_range), then the per-ray radii
+    of every variant are all-gathered (sharded_radii) -- the scan's one
+    exchange; wall time is the max over ranks, particle.turns the sum.  The
+    reference's analogue is the angle-parallel OpenMP scan
+    (bmad/modules/dynamic_aperture_mod.f90:182-196)."""
+    b, e = shard_range(n_variants, rank, world)
+    res = scan(b, e)
+    if world == 1:
+        return ShardedScan(res.radius, res, b, e, res.wall_s, res.particle_turns)
+    import torch
+    import torch.distributed as dist
+
+    full = sharded_radii(res.radius, n_variants, rank, world, group)
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    w = torch.tensor([res.wall_s], dtype=torch.float64, device=dev)
+    dist.all_reduce(w, op=dist.ReduceOp.MAX, group=group)
+    pt = torch.tensor([float(res.particle_turns)], dtype=torch.float64, device=dev)
+    dist.all_reduce(pt, op=dist.ReduceOp.SUM, group=group)
+    return ShardedScan(full, res, b, e, float(w.item()), int(pt.item()))

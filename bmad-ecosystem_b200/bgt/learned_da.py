@@ -7,11 +7,17 @@ then reads the start coordinates, the variant's lattice-error summary, and
 the coordinates and linear actions at turn `early`, and gives p(lost).
 Probes still alive at that turn are
 
-* retired as lost when p > p_hi (0.98) and as surviving when p < p_lo,
-* tracked to the full turn count by the FP64 tracker when p is in the
-  uncertainty band [p_lo, p_hi], when they lie within `boundary_cells` grid
-  cells of the predicted DA boundary of their ray, or when drawn into the
-  random audit fraction (2 %).
+* retired as lost when p > p_hi (0.98) -- the only early retirement the
+  method allows: "only particles it marks confidently as lost are retired
+  early";
+* tracked to the full turn count by the FP64 tracker otherwise: every probe
+  of the uncertainty band p <= p_hi, every probe within `boundary_cells`
+  grid cells of the predicted DA boundary of its ray, and a random audit
+  fraction (2 %) of the rest.
+
+`p_lo` > 0 (default 0) also retires confident survivors (p < p_lo) as
+surviving without tracking them: a faster scan outside that rule, kept as a
+measured comparison only.
 
 The DA radius of each ray then comes from the tracked outcomes where they
 exist and the classifier's labels elsewhere, and the audit measures the
@@ -240,6 +246,27 @@ def training_set(pb: ScanProblem, scans: Sequence[StagedScan], net: SurvivalMLP)
     return torch.cat(raws), torch.cat(labels)
 
 
+def gather_rows(t, group=None):
+    """Concatenate a [n_rank, ...] tensor over all ranks in rank order (rows
+    per rank may differ): the training samples of a scan sharded by variant,
+    so that every rank trains the same network on all of them."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        return t
+    world = dist.get_world_size(group)
+    n = torch.tensor([t.shape[0]], dtype=torch.int64, device=t.device)
+    ns = [torch.empty_like(n) for _ in range(world)]
+    dist.all_gather(ns, n, group=group)
+    ns = [int(x.item()) for x in ns]
+    buf = torch.zeros((max(ns),) + tuple(t.shape[1:]), dtype=t.dtype, device=t.device)
+    buf[:t.shape[0]] = t
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    return torch.cat([p[:k] for p, k in zip(parts, ns)])
+
+
 def normalized_inputs(net: SurvivalMLP, raw):
     """bf16 [pad_rows(n), 64] network inputs from raw features (n, 30)."""
     import torch
@@ -287,7 +314,7 @@ class PrunedResult:
 
 
 def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, early: int = 64,
-                n_turns: Optional[int] = None, p_hi: float = 0.98, p_lo: float = 0.02, audit: float = 0.02,
+                n_turns: Optional[int] = None, p_hi: float = 0.98, p_lo: float = 0.0, audit: float = 0.02,
                 boundary_cells: int = 2, seed: int = 0, retune_subset: bool = True) -> PrunedResult:
     """The kept probes are far fewer than the grid, so their tracking is
     bound by one particle's turn latency rather than by throughput; with
@@ -318,7 +345,7 @@ def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, ear
     first = torch.where(any_lost, g.int().argmax(dim=-1), torch.full_like(any_lost, nr, dtype=torch.int64))
     r_idx = torch.arange(nr, device=dev).view(1, 1, 1, nr)
     near = ((r_idx - first.unsqueeze(-1)).abs() <= boundary_cells).view(-1)
-    band = (p >= p_lo) & (p <= p_hi)
+    band = (p >= p_lo) & (p <= p_hi)  # p_lo = 0: every probe not confidently lost
     gen = torch.Generator(device="cpu").manual_seed(seed)
     aud = (torch.rand(n, generator=gen) < audit).to(dev)
     track_mask = alive & (band | near | aud)

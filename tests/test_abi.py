@@ -61,3 +61,38 @@ def test_struct_offsets_match_the_c_compiler(tmp_path):
         assert got[(st, "sizeof")] == ctypes.sizeof(cls), st
         for f in fields:
             assert got[(st, f)] == getattr(cls, f).offset, (st, f)
+
+
+def _fortran_type_fields(src: str, name: str):
+    """(field, kind, count) in declaration order of a bind(c) derived type
+    of the Fortran shim."""
+    body = re.search(rf"type, bind\(c\) :: {name}\n(.*?)\nend type", src, re.S).group(1)
+    out = []
+    for line in body.splitlines():
+        m = re.match(r"\s*(integer\(c_int32_t\)|real\(c_double\))\s*::\s*(.*)$", line)
+        if not m:
+            continue
+        kind = "i32" if "int32" in m.group(1) else "f64"
+        for f in re.split(r",\s*(?![^()]*\))", m.group(2)):
+            fm = re.match(r"(\w+)(?:\((\w+)\))?", f.strip())
+            out.append((fm.group(1), kind, 22 if fm.group(2) else 1))
+    return out
+
+
+def test_fortran_shim_mirrors_the_c_structs_and_symbols():
+    """The Fortran module (no compiler for it here) declares the C structs
+    field for field in the header's order and binds only exported symbols."""
+    import ctypes as C
+
+    src = (ROOT / "bmad-ecosystem_b200" / "fortran" / "bgt_mod.f90").read_text()
+    for fname, cls in (("bgt_element_c", _lib.BgtElement), ("bgt_species_c", _lib.BgtSpecies),
+                       ("bgt_tuning_c", _lib.BgtTuning)):
+        want = []
+        for f, t in cls._fields_:
+            if issubclass(t, C.Array):
+                want.append((f, "f64", t._length_))
+            else:
+                want.append((f, "i32" if t is C.c_int32 else "f64", 1))
+        assert _fortran_type_fields(src, fname) == want, fname
+    bound = set(re.findall(r"bind\(c, name='(bgt_\w+)'\)", src))
+    assert bound and bound <= set(declared_symbols())
