@@ -34,12 +34,13 @@ class BgtElement(C.Structure):
         ("coupler_angle", C.c_double), ("coupler_phase", C.c_double), ("fq1", C.c_double), ("fq2", C.c_double)] + [
         (n, C.c_double) for n in ("px_aperture_width2", "px_aperture_center", "py_aperture_width2",
                                   "py_aperture_center", "z_aperture_width2", "z_aperture_center",
-                                  "pz_aperture_width2", "pz_aperture_center")]
+                                  "pz_aperture_width2", "pz_aperture_center", "delta_ref_time", "ref_time_start")]
 
 
 class BgtSpecies(C.Structure):
     _fields_ = [("mass", C.c_double), ("charge", C.c_int32), ("aperture_limit_on", C.c_int32),
-                ("max_aperture_limit", C.c_double)]
+                ("max_aperture_limit", C.c_double), ("absolute_time_tracking", C.c_int32),
+                ("absolute_time_ref_shift", C.c_int32)]
 
 
 class BgtTuning(C.Structure):
@@ -87,11 +88,13 @@ def load() -> C.CDLL:
     lib.bgt_table_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
     lib.bgt_set_tuning.argtypes = [C.c_void_p, C.POINTER(BgtTuning)]
     lib.bgt_get_tuning.argtypes = [C.c_void_p, C.POINTER(BgtTuning)]
-    lib.bgt_track_turns.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _ip, C.c_int64, C.c_int32, C.c_int32]
+    lib.bgt_track_turns.argtypes = [C.c_void_p, _dp, _dp, C.c_void_p, _ip, _ip, _ip, _ip, C.c_int64, C.c_int32,
+                                    C.c_int32]
     lib.bgt_track_turns_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                           C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
+                                           C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p]
     lib.bgt_device_status.argtypes = [C.c_void_p, C.c_void_p]
-    lib.bgt_track_elements.argtypes = [C.c_void_p, _dp, _dp, _ip, _ip, _ip, C.c_int64, C.c_int32, C.c_int32]
+    lib.bgt_track_elements.argtypes = [C.c_void_p, _dp, _dp, C.c_void_p, _ip, _ip, _ip, C.c_int64, C.c_int32,
+                                       C.c_int32]
     lib.bgt_da_scan_grid.argtypes = [C.c_void_p, _dp, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                      C.c_int32, C.c_double, C.c_double, C.c_int32, _dp, _ip]
     lib.bgt_kernel_launch_count.argtypes = [C.c_void_p]
@@ -131,7 +134,7 @@ def to_bgt_element(e: L.Element) -> BgtElement:
               "y_offset", "z_offset", "x_pitch", "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick",
               "x1_limit", "x2_limit", "y1_limit", "y2_limit", "px_aperture_width2", "px_aperture_center",
               "py_aperture_width2", "py_aperture_center", "z_aperture_width2", "z_aperture_center",
-              "pz_aperture_width2", "pz_aperture_center"):
+              "pz_aperture_width2", "pz_aperture_center", "delta_ref_time", "ref_time_start"):
         setattr(b, n, e.v(n))
     if e.key in ("multipole", "ab_multipole"):
         _, knl, tn = L.multipole_ele_to_kt(e, True)

@@ -509,11 +509,25 @@ class Lattice:
     info: Dict[str, float] = field(default_factory=dict)
 
     def finalize(self) -> "Lattice":
+        ref_time = 0.0
         for i, e in enumerate(self.elements):
             e.ix_ele = i + 1
             e.values["p0c"] = self.p0c
             e.values["e_tot"] = self.e_tot
             bookkeeper(e)
+            # reference time at the entrance and through the element, as
+            # lat_compute_reference_energy.f90 computes them for an element
+            # with a constant reference velocity (:743-748: delta_ref_time =
+            # l * E_tot / (p0c * c_light), 0 for zero length; ref_time =
+            # ref_time_start + delta_ref_time).  For an rfcavity Bmad tracks
+            # the reference particle instead (:750-753), which gives the same
+            # time up to rounding when the cavity does not change the
+            # reference energy; a caller with Bmad passes Bmad's own values.
+            e.values["ref_time_start"] = ref_time
+            ln = e.v("l")
+            dt = 0.0 if (ln == 0 or e.key == "marker") else ln * self.e_tot / (self.p0c * C_LIGHT)
+            e.values["delta_ref_time"] = dt
+            ref_time = ref_time + dt
         return self
 
     @property

@@ -25,25 +25,29 @@ import numpy as np
 
 from . import _lib
 from . import lattice as L
+from . import qp
 
 
 @dataclass
 class Bunch:
     """n particles: vec6[6, n] = (x, px, y, py, z, pz), beta[n], state[n],
-    ix_ele_lost[n], ix_turn_lost[n]."""
+    ix_ele_lost[n], ix_turn_lost[n], and optionally the particle times t
+    (binary128, an (n, 2) uint64 array: see bgt.qp)."""
 
     vec6: np.ndarray
     beta: np.ndarray
     state: np.ndarray
     ix_ele_lost: np.ndarray
     ix_turn_lost: np.ndarray
+    t: Optional[np.ndarray] = None
 
     @classmethod
-    def from_vec(cls, vec6: np.ndarray, p0c: float, mass: float) -> "Bunch":
+    def from_vec(cls, vec6: np.ndarray, p0c: float, mass: float, with_time: bool = False) -> "Bunch":
         v = np.ascontiguousarray(np.asarray(vec6, dtype=np.float64).reshape(6, -1))
         n = v.shape[1]
-        return cls(v, L.beta_of(p0c, v[5], mass), np.full(n, L.ALIVE, np.int32), np.full(n, -1, np.int32),
-                   np.full(n, -1, np.int32))
+        beta = L.beta_of(p0c, v[5], mass)
+        t = qp.initial_time(v, beta) if with_time else None
+        return cls(v, beta, np.full(n, L.ALIVE, np.int32), np.full(n, -1, np.int32), np.full(n, -1, np.int32), t)
 
     @property
     def n(self) -> int:
@@ -51,7 +55,12 @@ class Bunch:
 
     def copy(self) -> "Bunch":
         return Bunch(self.vec6.copy(), self.beta.copy(), self.state.copy(), self.ix_ele_lost.copy(),
-                     self.ix_turn_lost.copy())
+                     self.ix_turn_lost.copy(), None if self.t is None else self.t.copy())
+
+    @property
+    def time(self) -> np.ndarray:
+        """The particle times rounded to double."""
+        return qp.to_double(self.t)
 
     @property
     def n_live(self) -> int:
@@ -66,10 +75,12 @@ def _check(lib, h, rc, what):
 
 class Tracker:
     """Device element tables for one ring and any number of variants of it
-    (same element sequence, per-variant values)."""
+    (same element sequence, per-variant values).  absolute_time sets
+    bmad_com%absolute_time_tracking: the RF phase from the particle time,
+    which every bunch then carries."""
 
     def __init__(self, lattices: Union[L.Lattice, Sequence[L.Lattice]], device: int = 0,
-                 tuning: Optional[dict] = None):
+                 tuning: Optional[dict] = None, absolute_time: bool = False, absolute_time_ref_shift: bool = True):
         lats: List[L.Lattice] = [lattices] if isinstance(lattices, L.Lattice) else list(lattices)
         if not lats:
             raise ValueError("no lattice")
@@ -90,7 +101,9 @@ class Tracker:
                 if c is None:
                     c = seen[k] = _lib.to_bgt_element(e)
                 arr[v * n_ele + i] = c
-        sp = _lib.BgtSpecies(lats[0].species.mass, lats[0].species.charge, 1, 1e3)
+        sp = _lib.BgtSpecies(lats[0].species.mass, lats[0].species.charge, 1, 1e3, 1 if absolute_time else 0,
+                             1 if absolute_time_ref_shift else 0)
+        self.absolute_time = bool(absolute_time)
         self.species = lats[0].species
         self.p0c = lats[0].p0c
         h = C.c_void_p()
@@ -125,8 +138,19 @@ class Tracker:
         return int(self.lib.bgt_kernel_launch_count(self.h))
 
     # -- tracking ---------------------------------------------------------
-    def make_bunch(self, vec6) -> Bunch:
-        return Bunch.from_vec(vec6, self.p0c, self.species.mass)
+    def make_bunch(self, vec6, with_time: Optional[bool] = None) -> Bunch:
+        """A bunch at the ring start; with_time (default: with absolute time
+        tracking) gives it init_coord's particle times."""
+        wt = self.absolute_time if with_time is None else with_time
+        return Bunch.from_vec(vec6, self.p0c, self.species.mass, with_time=wt)
+
+    @staticmethod
+    def _t_ptr(b: Bunch):
+        if b.t is None:
+            return None
+        if b.t.shape != (b.n, 2) or b.t.dtype != np.uint64 or not b.t.flags["C_CONTIGUOUS"]:
+            raise ValueError("bunch.t must be a C-contiguous (n, 2) uint64 array of binary128 times")
+        return b.t.ctypes.data
 
     def track_turns(self, bunch: Bunch, n_turns: int, turn0: int = 0,
                     variant: Optional[np.ndarray] = None) -> Bunch:
@@ -138,7 +162,8 @@ class Tracker:
             if var.shape != (b.n,):
                 raise ValueError("variant must have one entry per particle")
         rc = self.lib.bgt_track_turns(self.h, _lib.ptr(b.vec6, C.c_double), _lib.ptr(b.beta, C.c_double),
-                                      _lib.ptr(b.state, C.c_int32), _lib.ptr(b.ix_ele_lost, C.c_int32),
+                                      self._t_ptr(b), _lib.ptr(b.state, C.c_int32),
+                                      _lib.ptr(b.ix_ele_lost, C.c_int32),
                                       _lib.ptr(b.ix_turn_lost, C.c_int32),
                                       _lib.ptr(var, C.c_int32) if var is not None else None, b.n, turn0, n_turns)
         _check(self.lib, self.h, rc, "bgt_track_turns")
@@ -150,7 +175,8 @@ class Tracker:
         b = bunch
         var = None if variant is None else np.ascontiguousarray(variant, dtype=np.int32)
         rc = self.lib.bgt_track_elements(self.h, _lib.ptr(b.vec6, C.c_double), _lib.ptr(b.beta, C.c_double),
-                                         _lib.ptr(b.state, C.c_int32), _lib.ptr(b.ix_ele_lost, C.c_int32),
+                                         self._t_ptr(b), _lib.ptr(b.state, C.c_int32),
+                                         _lib.ptr(b.ix_ele_lost, C.c_int32),
                                          _lib.ptr(var, C.c_int32) if var is not None else None, b.n, e_begin,
                                          e_end)
         _check(self.lib, self.h, rc, "bgt_track_elements")
@@ -161,11 +187,13 @@ class Tracker:
         return self.track_elements(bunch, position, position + 1, variant)
 
     def track_turns_device(self, vec6, beta, state, ix_ele_lost, ix_turn_lost, n_turns: int, turn0: int = 0,
-                           stream=None, variant=None):
+                           stream=None, variant=None, t=None):
         """Track device-resident torch tensors in place, enqueued on `stream`
         (a torch.cuda.Stream; default: the current stream).  `variant` (int32
         CUDA tensor, sorted) selects each particle's lattice variant; with
-        more than one variant the call synchronises the stream once."""
+        more than one variant the call synchronises the stream once.  `t`
+        (a contiguous (n, 2) int64 CUDA tensor of binary128 bits) carries the
+        particle times."""
         import torch
 
         if stream is None:
@@ -180,7 +208,10 @@ class Tracker:
         n = beta.numel()
         if vec6.numel() != 6 * n or (variant is not None and variant.numel() != n):
             raise ValueError("vec6 must hold 6*n values and variant n")
-        rc = self.lib.bgt_track_turns_device(self.h, vec6.data_ptr(), beta.data_ptr(), state.data_ptr(),
+        if t is not None and (not t.is_cuda or t.dtype != torch.int64 or not t.is_contiguous() or t.numel() != 2 * n):
+            raise ValueError("t must be a contiguous (n, 2) int64 CUDA tensor of binary128 bits")
+        rc = self.lib.bgt_track_turns_device(self.h, vec6.data_ptr(), beta.data_ptr(),
+                                             t.data_ptr() if t is not None else None, state.data_ptr(),
                                              ix_ele_lost.data_ptr(), ix_turn_lost.data_ptr(),
                                              variant.data_ptr() if variant is not None else None, n, turn0,
                                              n_turns, C.c_void_p(stream.cuda_stream))

@@ -570,6 +570,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       q[Q_RHALF] = r_step / 2;
       q[Q_RSTEP] = r_step;
       put_lez(q + Q_LEZ, e, sp.mass, p0c);
+      q[Q_DTREF] = e.delta_ref_time;
       h.n_step = n_step;
       h.ix_mag_max = ix;
       break;
@@ -584,6 +585,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       q[TM_STEP] = step_len;
       q[TM_RHALF] = 1 * r_step / 2;
       q[TM_RSTEP] = 1 * r_step;
+      q[TM_DTREF] = e.delta_ref_time;
       h.n_step = n_step;
       h.ix_mag_max = ix;
       break;
@@ -625,7 +627,9 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
         double hi = (double)amp;
         q[RF_HALF_AMP_HI] = hi;
         q[RF_HALF_AMP_LO] = (double)(amp - (__float128)hi);
+        memcpy(q + RF_AMPQ, &amp, 16);
       }
+      q[RF_TSTART] = e.ref_time_start;
       q[RF_PHI0_MP] = TWOPI_H * e.phi0_multipass;
       q[RF_RHALF] = 0.5 * r_step;
       // rf_coupler_kick.f90:41-60: e_accel_field(ele, gradient$) is voltage / l
@@ -729,6 +733,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       if (!edges && ixe > -1) flags |= F_NO_HWANG;
       put_edge(q + B_EDGE, e, true);
       put_edge(q + B_EDGE + EDGE_N, e, false);
+      q[B_DTREF] = e.delta_ref_time;
       // bend_edge_kick (fringe_mod.f90:39-127): the Hwang map for basic_bend,
       // hard_edge_only and sad_full; the SAD soft edge for soft_edge_only and
       // sad_full (nothing when fint hgap or g + dg is zero); the linear edge;

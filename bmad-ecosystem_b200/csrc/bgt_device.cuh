@@ -9,6 +9,7 @@
 #include <stdint.h>
 
 #include "bgt_crmath.cuh"
+#include "bgt_qp.cuh"
 #include "bgt_table.h"
 
 // Every transcendental of a particle coordinate goes through bgt::cr
@@ -32,12 +33,27 @@ struct Glob {
   double mal;       // bmad_com%max_aperture_limit
   int32_t ap_on;    // bmad_com%aperture_limit_on
   int32_t charge;
+  int32_t abs_time;       // bmad_com%absolute_time_tracking
+  int32_t abs_ref_shift;  // bmad_com%absolute_time_ref_shift
+  int32_t track_time;     // the particle time t is carried (the kernel sets 0 in instances without it)
 };
 
+// A particle: phase-space coordinates, beta, state and the time t as
+// binary128 bits (the reference's real(qp) coord_struct%t), advanced only
+// when Glob::track_time is set.
 struct Part {
   double x, px, y, py, z, pz, beta;
   int32_t state;
+  uint64_t t_lo, t_hi;
 };
+
+__device__ __forceinline__ qp::Q time_of(const Part& p) { return qp::Q{p.t_lo, p.t_hi}; }
+__device__ __forceinline__ void set_time(Part& p, qp::Q t) {
+  p.t_lo = t.lo;
+  p.t_hi = t.hi;
+}
+// t = t + dt, dt a real(rp) step, the sum rounded in real(qp)
+__device__ __forceinline__ void add_time(Part& p, double dt) { set_time(p, qp::add(time_of(p), qp::from_double(dt))); }
 
 // Per-particle memo of the drift's pz-only term (track_a_drift.f90:69,
 // first sqrt_one).  Value-identical: recomputed whenever pz differs.
@@ -388,7 +404,19 @@ __device__ __forceinline__ void track_a_drift(Part& p, double length, const Glob
       dz = -length / ps_rel;
     }
   }
+  // dt = rel_z_vel * length / (beta * ps_rel * c_light); t = t + dt
+  // (track_a_drift.f90:79-80)
+  if (G.track_time && p.beta > 0) add_time(p, length / (p.beta * ps_rel * C_LIGHT));
   p.z = p.z + dz;
+}
+
+// t = start t + delta_ref_time + (start z - z) / (beta * c_light), summed
+// left to right in real(qp) (track_a_quadrupole.f90:144,
+// track_a_bend.f90:327, track_a_thick_multipole.f90:133).
+__device__ __forceinline__ void element_exit_time(Part& p, qp::Q t0, double z0, double dt_ref, const Glob& G) {
+  if (!G.track_time) return;
+  const double dz_t = (z0 - p.z) / (p.beta * C_LIGHT);
+  set_time(p, qp::add(qp::add(t0, qp::from_double(1 * dt_ref)), qp::from_double(dz_t)));
 }
 
 // bmad/code/tilt_coords.f90:18-53 with host-evaluated cos/sin of the angle

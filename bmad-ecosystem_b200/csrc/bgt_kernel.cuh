@@ -95,6 +95,8 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
   const double* be = ae + (ixe + 1);
   const double* hard = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);
   const double* soft = hard + ((fl & F_HARD_EDGE) ? 1 : 0);
+  const qp::Q t0 = time_of(p);  // start_orb = orbit (track_a_quadrupole.f90:40)
+  const double z0 = p.z;
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
   if (RARE && (fl & F_FRINGE_INFO)) {
     // apply_element_edge_kick.f90:160-176, first edge: magnetic (hard, then
@@ -157,6 +159,7 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
     if (p.state != ALIVE) return;
   }
   if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
+  element_exit_time(p, t0, z0, q[Q_DTREF], G);
 }
 
 // bmad/low_level/track_a_thick_multipole.f90:18-134
@@ -172,6 +175,8 @@ __device__ __forceinline__ void body_thick(Part& p, const Rec& R, const Glob& G,
   const double* ae = an + 2 * (ix + 1);
   const double* be = ae + (ixe + 1);
   const double* hard = ae + ((fl & F_ELEC) ? 2 * (ixe + 1) : 0);
+  const qp::Q t0 = time_of(p);  // start_orb = orbit (track_a_thick_multipole.f90:41)
+  const double z0 = p.z;
   if (fl & F_MISALIGN) offset_set(p, R.mis, fl, G, m, true);
   if (RARE && (fl & F_FRINGE_INFO)) {
     if (fl & F_EDGE_IN) {
@@ -195,6 +200,7 @@ __device__ __forceinline__ void body_thick(Part& p, const Rec& R, const Glob& G,
     if (p.state != ALIVE) return;
   }
   if (fl & F_MISALIGN) offset_unset(p, R.mis, fl, G, m, true);
+  element_exit_time(p, t0, z0, q[TM_DTREF], G);
 }
 
 // multipole_kick, bmad/modules/multipole_mod.f90:203-286
@@ -324,15 +330,35 @@ __device__ __forceinline__ void body_rf(Part& p, const Rec& R, const Glob& G, Dr
   if (ix > -1) ab_multipole_kicks(p, an, bn, ix, q[RF_RHALF]);
   const double voltage = q[RF_VOLT];
   const double f = q[RF_FREQ];
-  // particle_rf_time, relative time: time = -z / (beta * c_light)
-  double time = -p.z / (p.beta * C_LIGHT);
-  DD t = {time, 0.0};
-  if (f != 0) t = dd_modulo2(time, DD{q[RF_HALF_AMP_HI], q[RF_HALF_AMP_LO]});
-  DD tf = dd_mul_d(t, f);
-  DD u = dd_add({q[RF_PHI0], 0.0}, dd_neg(tf));
-  DD v = dd_mul_d(u, TWOPI_D);
-  double phase0 = v.hi + v.lo;
-  phase0 = phase0 + q[RF_PHI0_MP];
+  double phase0;
+  if (RARE && G.abs_time) {
+    // particle_rf_time, absolute time (particle_rf_time.f90:74-76): t less
+    // the cavity's ref_time_start, folded by modulo2 and multiplied out in
+    // real(qp) (:116-118, track_a_rfcavity.f90:78-80) with the binary128
+    // arithmetic of bgt_qp.cuh, then rounded to real(rp); no phi0_multipass
+    // (:81)
+    qp::Q time = time_of(p);
+    if (G.abs_ref_shift) time = qp::sub(time, qp::from_double(q[RF_TSTART]));
+    if (f != 0) {
+      qp::Q amp;
+      memcpy(&amp, q + RF_AMPQ, 16);
+      time = qp::modulo2(time, amp);
+    }
+    const qp::Q ph = qp::mul(qp::from_double(TWOPI_D),
+                             qp::sub(qp::from_double(q[RF_PHI0]),
+                                     qp::mul(qp::sub(time, qp::from_double(0.0)), qp::from_double(f))));
+    phase0 = qp::to_double(ph);
+  } else {
+    // particle_rf_time, relative time: time = -z / (beta * c_light)
+    double time = -p.z / (p.beta * C_LIGHT);
+    DD t = {time, 0.0};
+    if (f != 0) t = dd_modulo2(time, DD{q[RF_HALF_AMP_HI], q[RF_HALF_AMP_LO]});
+    DD tf = dd_mul_d(t, f);
+    DD u = dd_add({q[RF_PHI0], 0.0}, dd_neg(tf));
+    DD v = dd_mul_d(u, TWOPI_D);
+    phase0 = v.hi + v.lo;
+    phase0 = phase0 + q[RF_PHI0_MP];
+  }
   // modulo2(phase0, pi) in double
   double per = 2 * PI_D;
   double mod = fmod(phase0, per);
@@ -530,6 +556,8 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
   const int ixe = RARE ? R.h->aux1 : -1;
   const double* ae = an + 2 * (ix + 1);
   const double* be = ae + (ixe + 1);
+  const qp::Q t0 = time_of(p);  // start_orb = orbit (track_a_bend.f90:42)
+  const double z0 = p.z;
   if (fl & F_MISALIGN) {
     if (RARE && (fl & F_BEND_MIS))
       bend_offset(p, R.mis + MIS_N, true, R.mis[MIS_LHALF], G, m);
@@ -637,6 +665,7 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
     else
       offset_unset(p, R.mis, fl, G, m, true);
   }
+  element_exit_time(p, t0, z0, q[B_DTREF], G);
 }
 
 // track1, bmad/code/track1.f90:43-342 for one alive particle and one record:
@@ -742,6 +771,7 @@ struct KArgs {
   int32_t* state;
   int32_t* ix_ele_lost;
   int32_t* ix_turn_lost;
+  uint64_t* t;                   // particle times, binary128 bits [n][2] (nullptr = not tracked; RARE only)
   const int32_t* slot_particle;  // slot -> particle index, -1 = padding (nullptr = identity)
   const int32_t* tile_variant;   // tile -> variant (nullptr = variant 0)
   int64_t n;                     // particles
@@ -767,6 +797,23 @@ struct KArgs {
 
 constexpr int MAX_BLOCK = 256;
 
+// Particle time in and out of global memory, binary128 bits per particle
+// (t[2 i], t[2 i + 1]); only the kernel instances that track time touch them.
+template <bool RARE>
+__device__ __forceinline__ void load_time(Part& p, const uint64_t* t, int64_t i) {
+  if (RARE && t) {
+    p.t_lo = t[2 * i];
+    p.t_hi = t[2 * i + 1];
+  }
+}
+template <bool RARE>
+__device__ __forceinline__ void store_time(const Part& p, uint64_t* t, int64_t i) {
+  if (RARE && t) {
+    t[2 * i] = p.t_lo;
+    t[2 * i + 1] = p.t_hi;
+  }
+}
+
 // TMODE 0: the variant's element table is staged in shared memory.
 // TMODE 1: it is read from global memory (L2 / L1) instead -- for tables
 //   larger than the shared-memory budget (e.g. every quadrupole and sextupole
@@ -791,12 +838,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
   __shared__ int32_t s_warp_cnt[BLOCK / 32];
   const double* table = smem;
   // compaction staging area sits after the table
-  double* stage = smem + (GTAB ? 0 : a.table_dw);  // [9][BLOCK] doubles; rows 7-8 hold int32 ids and loss records
-  int32_t* stage_i = reinterpret_cast<int32_t*>(stage + 7 * BLOCK);  // [3][BLOCK]
+  // [STAGE_ROWS][BLOCK] doubles; rows 7-8 hold int32 ids and loss records,
+  // rows 9-10 the particle times (RARE)
+  constexpr int STAGE_ROWS = RARE ? 11 : 9;
+  double* stage = smem + (GTAB ? 0 : a.table_dw);
+  int32_t* stage_i = reinterpret_cast<int32_t*>(stage + 7 * BLOCK);   // [3][BLOCK]
+  uint64_t* stage_t = reinterpret_cast<uint64_t*>(stage + 9 * BLOCK);  // [2][BLOCK]
   // quad memo after the (optional) compaction stage
-  double* qmemo_base = stage + (a.compact_every > 0 ? 9 * BLOCK : 0);
+  double* qmemo_base = stage + (a.compact_every > 0 ? STAGE_ROWS * BLOCK : 0);
   const QMemo qmemo{qmemo_base + threadIdx.x, BLOCK};
 
+  // the instances without time tracking (RARE = false) never carry the
+  // particle time: track_time = 0 is then a constant and the time arithmetic
+  // is compiled out
+  Glob G = a.G;
+  if (!RARE) G.track_time = 0;
   const int tid = threadIdx.x;
   if (TMODE == 2) {
     // Tables in global memory: no CTA-wide state to share, so every warp
@@ -822,6 +878,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
       Part p;
       int32_t ixe = -1, ixt = -1;
       p.state = 0;
+      p.t_lo = 0;
+      p.t_hi = 0;
       if (pidx >= 0) {
         p.x = a.vec6[0 * a.n_stride + pidx];
         p.px = a.vec6[1 * a.n_stride + pidx];
@@ -833,13 +891,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
         p.state = a.state[pidx];
         ixe = a.ix_ele_lost[pidx];
         if (a.ix_turn_lost) ixt = a.ix_turn_lost[pidx];
+        load_time<RARE>(p, a.t, pidx);
       }
       DriftMemo memo;
       memo.pz = NAN;
       memo.a = 0;
 #pragma unroll
       for (int c = 0; c < QMEMO_CLASSES; c++) qmemo.q[(c * 13 + 12) * qmemo.stride] = NAN;
-      if (p.state == ALIVE && orbit_too_large(p, a.G)) {
+      if (p.state == ALIVE && orbit_too_large(p, G)) {
         ixe = wseq[a.rec_begin].y;
         ixt = a.turn0;
       }
@@ -849,7 +908,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
         for (int r = a.rec_begin; r < a.rec_end; r++) {
           const int2 e = wseq[r];
           if (p.state == ALIVE) {
-            track1_rec<RARE>(p, wtable + e.x, a.G, memo, qmemo);
+            track1_rec<RARE>(p, wtable + e.x, G, memo, qmemo);
             if (p.state != ALIVE) {
               ixe = e.y;
               ixt = turn;
@@ -868,6 +927,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
         a.state[pidx] = p.state;
         a.ix_ele_lost[pidx] = ixe;
         if (a.ix_turn_lost) a.ix_turn_lost[pidx] = ixt;
+        store_time<RARE>(p, a.t, pidx);
       }
     }
     return;
@@ -917,6 +977,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
     Part p;
     int32_t ixe = -1, ixt = -1;
     p.state = 0;
+    p.t_lo = 0;
+    p.t_hi = 0;
     if (pidx >= 0) {
       p.x = a.vec6[0 * a.n_stride + pidx];
       p.px = a.vec6[1 * a.n_stride + pidx];
@@ -928,6 +990,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
       p.state = a.state[pidx];
       ixe = a.ix_ele_lost[pidx];
       if (a.ix_turn_lost) ixt = a.ix_turn_lost[pidx];
+      load_time<RARE>(p, a.t, pidx);
     }
     DriftMemo memo;
     memo.pz = NAN;
@@ -939,7 +1002,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
     // entrance check of the first element (check_aperture_limit ->
     // orbit_too_large, track1.f90:195)
     if (p.state == ALIVE) {
-      if (orbit_too_large(p, a.G)) {
+      if (orbit_too_large(p, G)) {
         ixe = seq[a.rec_begin].y;
         ixt = a.turn0;
       }
@@ -954,7 +1017,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
         for (int r = a.rec_begin; r < a.rec_end; r++) {
           const int2 e = seq[r];
           if (p.state == ALIVE) {
-            track1_rec<RARE>(p, table + e.x, a.G, memo, qmemo);
+            track1_rec<RARE>(p, table + e.x, G, memo, qmemo);
             if (p.state != ALIVE) {
               ixe = e.y;
               ixt = turn;
@@ -990,6 +1053,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
             a.state[my_idx] = p.state;
             a.ix_ele_lost[my_idx] = ixe;
             if (a.ix_turn_lost) a.ix_turn_lost[my_idx] = ixt;
+            store_time<RARE>(p, a.t, my_idx);
           }
           const int dst = base + __popc(ballot & ((1u << lane) - 1u));
           if (alive) {
@@ -1003,6 +1067,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
             stage_i[dst] = my_idx;
             stage_i[BLOCK + dst] = ixe;
             stage_i[2 * BLOCK + dst] = ixt;
+            if (RARE) {
+              stage_t[dst] = p.t_lo;
+              stage_t[BLOCK + dst] = p.t_hi;
+            }
           }
           __syncthreads();
           if (tid < total) {
@@ -1016,6 +1084,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
             my_idx = stage_i[tid];
             ixe = stage_i[BLOCK + tid];
             ixt = stage_i[2 * BLOCK + tid];
+            if (RARE) {
+              p.t_lo = stage_t[tid];
+              p.t_hi = stage_t[BLOCK + tid];
+            }
             p.state = ALIVE;
             memo.pz = NAN;
 #pragma unroll
@@ -1041,6 +1113,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) track_kernel(KArgs a) {
       a.state[my_idx] = p.state;
       a.ix_ele_lost[my_idx] = ixe;
       if (a.ix_turn_lost) a.ix_turn_lost[my_idx] = ixt;
+      store_time<RARE>(p, a.t, my_idx);
     }
     __syncthreads();
   }

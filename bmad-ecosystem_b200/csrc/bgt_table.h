@@ -160,11 +160,12 @@ constexpr int Q_STEP = 2;     // step_len
 constexpr int Q_RHALF = 3;    // r_step / 2
 constexpr int Q_RSTEP = 4;    // r_step
 constexpr int Q_LEZ = 5;      // low_energy_z_correction constants, LEZ_N doubles
-constexpr int Q_N = Q_LEZ + 6;
+constexpr int Q_DTREF = Q_LEZ + 6;  // delta_ref_time
+constexpr int Q_N = Q_DTREF + 1;
 constexpr int LEZ_BETA0 = 0, LEZ_MB2_THRESH = 1, LEZ_F = 2, LEZ_ME2 = 3, LEZ_MASS = 4, LEZ_3E7 = 5;
 
-// Thick multipole: step_len, r_step/2, r_step
-constexpr int TM_STEP = 0, TM_RHALF = 1, TM_RSTEP = 2, TM_N = 3;
+// Thick multipole: step_len, r_step/2, r_step, delta_ref_time
+constexpr int TM_STEP = 0, TM_RHALF = 1, TM_RSTEP = 2, TM_DTREF = 3, TM_N = 4;
 
 // Bend
 constexpr int B_LEN = 0, B_G = 1, B_DG = 2, B_GTOT = 3, B_STEP = 4, B_ANGLE = 5, B_RSTEP = 6;
@@ -186,7 +187,8 @@ constexpr int B_EDGE = B_K1 + 3;  // Hwang edge constants, entrance block then e
 constexpr int EDGE_GT = 0, EDGE_GT2 = 1, EDGE_GS2 = 2, EDGE_K1TANE = 3, EDGE_K1TANE2 = 4, EDGE_FG = 5,
               EDGE_C1 = 6, EDGE_C3 = 7, EDGE_C4 = 8, EDGE_GPG = 9, EDGE_GTGS2_2K1 = 10;
 constexpr int EDGE_N = 11;
-constexpr int B_N = B_EDGE + 2 * EDGE_N;
+constexpr int B_DTREF = B_EDGE + 2 * EDGE_N;  // delta_ref_time
+constexpr int B_N = B_DTREF + 1;
 
 // Exact bend edge block (F_EXACT_EDGE, exact_bend_edge_kick,
 // fringe_mod.f90:1465-1686): beta0 = p0c / e_tot, 1 / beta0,
@@ -214,7 +216,9 @@ constexpr int RF_PHI0_MP = 9;  // twopi * phi0_multipass
 constexpr int RF_RHALF = 10;   // 0.5 * r_step (multipole kicks)
 constexpr int RF_CPL_DPX = 11, RF_CPL_DPY = 12;  // coupler dp_x, dp_y (halved for both ends)
 constexpr int RF_CPL_PH = 13;  // twopi * coupler_phase
-constexpr int RF_N = 14;
+constexpr int RF_TSTART = 14;  // ref_time_start (absolute time)
+constexpr int RF_AMPQ = 15;    // 0.5/f in real(qp): binary128 bits in two doubles (absolute time)
+constexpr int RF_N = 17;
 
 // Multipole arrays for quad / bend / thick multipole / rf follow the kind
 // block: an[0..ix_mag_max], bn[0..ix_mag_max].

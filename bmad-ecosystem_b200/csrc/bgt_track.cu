@@ -40,6 +40,7 @@ struct CallCtx {
   double* d_vec6 = nullptr;
   double* d_beta = nullptr;
   int32_t* d_i32 = nullptr;  // state, ixe, ixt, slot map, tile variant
+  uint64_t* d_t = nullptr;   // particle times (binary128), cap of them
   int64_t cap = 0, cap_slots = 0, cap_tiles = 0;
   // pinned host staging of host-buffer calls
   unsigned char* h_pin = nullptr;
@@ -109,6 +110,7 @@ static void free_ctx(CallCtx* c) {
   cudaFree(c->d_vec6);
   cudaFree(c->d_beta);
   cudaFree(c->d_i32);
+  cudaFree(c->d_t);
   cudaFree(c->d_grp);
   cudaFree(c->d_grp_v);
   if (c->h_pin) cudaFreeHost(c->h_pin);
@@ -168,9 +170,12 @@ static bgt_tuning get_tuning_locked(bgt_handle* h) {
   return h->tuning;
 }
 
-static size_t smem_bytes(const bgt_handle* h, int block, bool compact, bool gtab = false) {
+// Dynamic shared memory of a launch: the table (unless read from global
+// memory), the compaction stage (9 rows of BLOCK doubles, 11 with the
+// particle times of the RARE instances) and the quadrupole memo.
+static size_t smem_bytes(const bgt_handle* h, int block, bool compact, bool gtab, bool rare) {
   size_t b = gtab ? 0 : (size_t)h->table_dw * 8;
-  if (compact) b += (size_t)9 * block * 8;
+  if (compact) b += (size_t)(rare ? 11 : 9) * block * 8;
   b += (size_t)QMEMO_CLASSES * 13 * block * 8;
   return b;
 }
@@ -234,16 +239,17 @@ static uint64_t wait_ns_of(const bgt_tuning& t) {
 
 // The kernel instance for a tuning and a shared-memory need, with the
 // placement of the table it implies; 0 or an error code.
-static int pick_kernel(bgt_handle* h, const bgt_tuning& tun, bool compact, LaunchFn* fn, size_t* smem) {
+static int pick_kernel(bgt_handle* h, const bgt_tuning& tun, bool compact, bool rare, LaunchFn* fn,
+                       size_t* smem) {
   const int block = tun.threads_per_block;
-  const bool fits = smem_bytes(h, block, compact) <= SMEM_LIMIT;
+  const bool fits = smem_bytes(h, block, compact, false, rare) <= SMEM_LIMIT;
   if (tun.table_mode == 1 && !fits)
     return set_err(h, BGT_ETOOLARGE, "element table does not fit in shared memory (table_mode 1)");
   const bool gtab = tun.table_mode >= 2 || !fits;
   const bool warp_sched = tun.table_mode == 3;
-  *smem = smem_bytes(h, block, compact, gtab);
+  *smem = smem_bytes(h, block, compact, gtab, rare);
   if (*smem > SMEM_LIMIT) return set_err(h, BGT_ETOOLARGE, "tracking state does not fit in shared memory");
-  *fn = find_track_kernel(block, tun.blocks_per_sm, gtab ? (warp_sched ? 2 : 1) : 0, h->rare);
+  *fn = find_track_kernel(block, tun.blocks_per_sm, gtab ? (warp_sched ? 2 : 1) : 0, rare);
   if (!*fn) {
     if (gtab)
       return set_err(h, BGT_ETOOLARGE,
@@ -261,7 +267,9 @@ static int enqueue_track(bgt_handle* h, const bgt_tuning& tun, CallCtx* c, KArgs
                          cudaStream_t st) {
   LaunchFn launch = nullptr;
   size_t smem = 0;
-  int rc = pick_kernel(h, tun, a.compact_every > 0, &launch, &smem);
+  // the RARE instances also carry the particle time
+  const bool rare = h->rare || a.t != nullptr;
+  int rc = pick_kernel(h, tun, a.compact_every > 0, rare, &launch, &smem);
   if (rc) return rc;
   int64_t grid = (int64_t)h->num_sms * std::max(1, tun.blocks_per_sm);
   if (grid > n_tiles) grid = n_tiles;
@@ -323,6 +331,8 @@ int bgt_create(bgt_handle** out, const bgt_element* eles, int32_t n_ele, int32_t
   h->G.mal = species->max_aperture_limit;
   h->G.ap_on = species->aperture_limit_on;
   h->G.charge = species->charge;
+  h->G.abs_time = species->absolute_time_tracking ? 1 : 0;
+  h->G.abs_ref_shift = species->absolute_time_ref_shift ? 1 : 0;
   std::vector<double> all;
   std::string msg;
   int rc = host::compile_tables(eles, n_ele, n_variants, *species, QMEMO_CLASSES, all, h->h_table_off,
@@ -398,13 +408,16 @@ int64_t bgt_kernel_launch_count(const bgt_handle* h) { return h ? h->launches.lo
 // segments of tuning.turns_per_launch turns (one persistent launch each).
 // The call's error flag is cleared once, the tile counter per launch.
 static int track_device_impl(bgt_handle* h, const bgt_tuning& tun, CallCtx* c, int32_t* status, double* d_vec6,
-                             int64_t n_stride, double* d_beta, int32_t* d_state, int32_t* d_ixe, int32_t* d_ixt,
+                             int64_t n_stride, double* d_beta, uint64_t* d_t, int32_t* d_state, int32_t* d_ixe,
+                             int32_t* d_ixt,
                              const int32_t* d_slot, const int32_t* d_tile_var, int64_t n, int64_t n_slots,
                              int32_t turn0, int32_t n_turns, int32_t rec_begin, int32_t rec_end, cudaStream_t st) {
   KArgs a = base_args(h, tun);
   a.vec6 = d_vec6;
   a.n_stride = n_stride;
   a.beta = d_beta;
+  a.t = d_t;
+  a.G.track_time = d_t ? 1 : 0;
   a.state = d_state;
   a.ix_ele_lost = d_ixe;
   a.ix_turn_lost = d_ixt;
@@ -452,11 +465,14 @@ __global__ void variant_slot_kernel(const int32_t* var, int64_t n, const int64_t
   slot[slot0[v] + (i - first[v])] = (int32_t)i;
 }
 
-int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state, int32_t* d_ix_ele_lost,
-                           int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n, int32_t turn0,
-                           int32_t n_turns, void* stream) {
+int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, void* d_t, int32_t* d_state,
+                           int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n,
+                           int32_t turn0, int32_t n_turns, void* stream) {
   if (!h || !d_vec6 || !d_beta || !d_state || !d_ix_ele_lost || n < 0 || n_turns < 0)
     return set_err(h, BGT_EINVAL, "bgt_track_turns_device: invalid argument");
+  if (h->G.abs_time && !d_t)
+    return set_err(h, BGT_EINVAL, "bgt_track_turns_device: absolute time tracking needs the particle times t");
+  uint64_t* tq = static_cast<uint64_t*>(d_t);
   if (n == 0 || n_turns == 0) return 0;
   if (n > INT32_MAX) return set_err(h, BGT_EINVAL, "bgt_track_turns_device: n exceeds 2^31 - 1");
   DeviceGuard dg(h->device);
@@ -469,8 +485,8 @@ int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_
   CallCtx* c = L.c;
   CU(h, L.use(st));
   if (!d_variant || h->n_variants == 1)
-    return track_device_impl(h, tun, c, h->d_status, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost,
-                             nullptr, nullptr, n, n, turn0, n_turns, 0, h->n_ele, st);
+    return track_device_impl(h, tun, c, h->d_status, d_vec6, n, d_beta, tq, d_state, d_ix_ele_lost,
+                             d_ix_turn_lost, nullptr, nullptr, n, n, turn0, n_turns, 0, h->n_ele, st);
   // Group by variant into tile-aligned slot ranges.  The variant ids must be
   // sorted (non-decreasing); the per-variant counts are read back once.
   const int32_t nv = h->n_variants;
@@ -517,7 +533,7 @@ int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_
   h->launches++;
   // (copies from pageable host memory return once the data is staged, so
   // slot0 and tvar may go out of scope before the copies complete)
-  return track_device_impl(h, tun, c, h->d_status, d_vec6, n, d_beta, d_state, d_ix_ele_lost, d_ix_turn_lost,
+  return track_device_impl(h, tun, c, h->d_status, d_vec6, n, d_beta, tq, d_state, d_ix_ele_lost, d_ix_turn_lost,
                            d_slot, d_tvar, n, n_slots, turn0, n_turns, 0, h->n_ele, st);
 }
 
@@ -543,21 +559,24 @@ int bgt_device_status(bgt_handle* h, void* stream) {
 }
 
 // Grow a context's device staging buffers.
-static int ensure_staging(bgt_handle* h, CallCtx* c, int64_t n, int64_t n_slots, int64_t n_tiles) {
-  if (n <= c->cap && n_slots <= c->cap_slots && n_tiles <= c->cap_tiles) return 0;
+static int ensure_staging(bgt_handle* h, CallCtx* c, int64_t n, int64_t n_slots, int64_t n_tiles, bool with_t) {
+  if (n <= c->cap && n_slots <= c->cap_slots && n_tiles <= c->cap_tiles && (!with_t || c->d_t)) return 0;
   CU(h, cudaStreamSynchronize(c->st));
   cudaFree(c->d_vec6);
   cudaFree(c->d_beta);
   cudaFree(c->d_i32);
+  cudaFree(c->d_t);
   c->d_vec6 = nullptr;
   c->d_beta = nullptr;
   c->d_i32 = nullptr;
+  c->d_t = nullptr;
   c->cap = std::max(n, c->cap);
   c->cap_slots = std::max(n_slots, c->cap_slots);
   c->cap_tiles = std::max(n_tiles, c->cap_tiles);
   CU(h, cudaMalloc(&c->d_vec6, (size_t)c->cap * 6 * 8));
   CU(h, cudaMalloc(&c->d_beta, (size_t)c->cap * 8));
   CU(h, cudaMalloc(&c->d_i32, (size_t)(3 * c->cap + c->cap_slots + c->cap_tiles) * 4));
+  if (with_t) CU(h, cudaMalloc(&c->d_t, (size_t)c->cap * 16));
   return 0;
 }
 
@@ -576,10 +595,11 @@ static int ensure_pinned(bgt_handle* h, CallCtx* c, size_t bytes) {
 // Host-buffer tracking shared by bgt_track_turns and bgt_track_elements: the
 // particles go through the context's pinned staging buffer to its device
 // buffers on its own stream; the call waits for that stream only.
-static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ixe, int32_t* ixt,
+static int track_host(bgt_handle* h, double* vec6, double* beta, void* t, int32_t* state, int32_t* ixe, int32_t* ixt,
                       const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns, int32_t rec_begin,
                       int32_t rec_end) {
   if (!h || !vec6 || !beta || !state || !ixe || n < 0) return set_err(h, BGT_EINVAL, "invalid argument");
+  if (h->G.abs_time && !t) return set_err(h, BGT_EINVAL, "absolute time tracking needs the particle times t");
   if (n == 0 || n_turns == 0) return 0;
   if (n > INT32_MAX) return set_err(h, BGT_EINVAL, "n exceeds 2^31 - 1");
   DeviceGuard dg(h->device);
@@ -619,13 +639,15 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
   CallCtx* c = L.c;
   cudaStream_t st = c->st;
   CU(h, L.use(st));
-  if ((rc = ensure_staging(h, c, n, n_slots, n_tiles))) return rc;
-  // pinned layout: vec6 [6][n], beta [n], state/ixe/ixt [n] each, slot map,
-  // tile variants, error flag
+  if ((rc = ensure_staging(h, c, n, n_slots, n_tiles, t != nullptr))) return rc;
+  // pinned layout: times [n][16 B] (when tracked), vec6 [6][n], beta [n],
+  // state/ixe/ixt [n] each, slot map, tile variants, error flag
+  const size_t b_t = t ? (size_t)n * 16 : 0;
   const size_t b_v = (size_t)n * 6 * 8, b_b = (size_t)n * 8, b_i = (size_t)n * 4;
   const size_t b_slot = multi ? (size_t)n_slots * 4 : 0, b_tv = multi ? tile_var.size() * 4 : 0;
-  if ((rc = ensure_pinned(h, c, b_v + b_b + 3 * b_i + b_slot + b_tv + 16))) return rc;
-  unsigned char* p = c->h_pin;
+  if ((rc = ensure_pinned(h, c, b_t + b_v + b_b + 3 * b_i + b_slot + b_tv + 16))) return rc;
+  unsigned char* p_time = c->h_pin;
+  unsigned char* p = c->h_pin + b_t;
   double* p_v = (double*)p;
   double* p_b = (double*)(p + b_v);
   int32_t* p_s = (int32_t*)(p + b_v + b_b);
@@ -634,6 +656,7 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
   int32_t* p_slot = p_t + n;
   int32_t* p_tv = p_slot + (multi ? n_slots : 0);
   int32_t* p_flag = p_tv + (multi ? tile_var.size() : 0);
+  if (t) memcpy(p_time, t, b_t);
   memcpy(p_v, vec6, b_v);
   memcpy(p_b, beta, b_b);
   memcpy(p_s, state, b_i);
@@ -648,6 +671,7 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
   int32_t* d_ixt = d_ixe + c->cap;
   int32_t* d_slot = d_ixt + c->cap;
   int32_t* d_tvar = d_slot + c->cap_slots;
+  if (t) CU(h, cudaMemcpyAsync(c->d_t, p_time, b_t, cudaMemcpyHostToDevice, st));
   CU(h, cudaMemcpy2DAsync(c->d_vec6, c->cap * 8, p_v, n * 8, n * 8, 6, cudaMemcpyHostToDevice, st));
   CU(h, cudaMemcpyAsync(c->d_beta, p_b, b_b, cudaMemcpyHostToDevice, st));
   CU(h, cudaMemcpyAsync(d_state, p_s, b_i, cudaMemcpyHostToDevice, st));
@@ -657,7 +681,8 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
     CU(h, cudaMemcpyAsync(d_slot, p_slot, b_slot, cudaMemcpyHostToDevice, st));
     CU(h, cudaMemcpyAsync(d_tvar, p_tv, b_tv, cudaMemcpyHostToDevice, st));
   }
-  rc = track_device_impl(h, tun, c, nullptr, c->d_vec6, c->cap, c->d_beta, d_state, d_ixe, ixt ? d_ixt : nullptr,
+  rc = track_device_impl(h, tun, c, nullptr, c->d_vec6, c->cap, c->d_beta, t ? c->d_t : nullptr, d_state, d_ixe,
+                         ixt ? d_ixt : nullptr,
                          multi ? d_slot : nullptr, multi ? d_tvar : nullptr, n, n_slots, turn0, n_turns, rec_begin,
                          rec_end, st);
   if (rc) {
@@ -665,6 +690,7 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
     return rc;
   }
   CU(h, cudaMemcpyAsync(p_flag, c->d_scratch + 1, 4, cudaMemcpyDeviceToHost, st));
+  if (t) CU(h, cudaMemcpyAsync(p_time, c->d_t, b_t, cudaMemcpyDeviceToHost, st));
   CU(h, cudaMemcpy2DAsync(p_v, n * 8, c->d_vec6, c->cap * 8, n * 8, 6, cudaMemcpyDeviceToHost, st));
   CU(h, cudaMemcpyAsync(p_b, c->d_beta, b_b, cudaMemcpyDeviceToHost, st));
   CU(h, cudaMemcpyAsync(p_s, d_state, b_i, cudaMemcpyDeviceToHost, st));
@@ -672,6 +698,7 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
   if (ixt) CU(h, cudaMemcpyAsync(p_t, d_ixt, b_i, cudaMemcpyDeviceToHost, st));
   CU(h, cudaStreamSynchronize(st));
   if (*p_flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete");
+  if (t) memcpy(t, p_time, b_t);
   memcpy(vec6, p_v, b_v);
   memcpy(beta, p_b, b_b);
   memcpy(state, p_s, b_i);
@@ -680,17 +707,17 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, int32_t* state,
   return 0;
 }
 
-int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, void* t, int32_t* state, int32_t* ix_ele_lost,
                     int32_t* ix_turn_lost, const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns) {
   if (!h) return set_err(nullptr, BGT_EINVAL, "null handle");
-  return track_host(h, vec6, beta, state, ix_ele_lost, ix_turn_lost, variant, n, turn0, n_turns, 0, h->n_ele);
+  return track_host(h, vec6, beta, t, state, ix_ele_lost, ix_turn_lost, variant, n, turn0, n_turns, 0, h->n_ele);
 }
 
-int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, void* t, int32_t* state, int32_t* ix_ele_lost,
                        const int32_t* variant, int64_t n, int32_t e_begin, int32_t e_end) {
   if (!h) return set_err(nullptr, BGT_EINVAL, "null handle");
   if (e_begin < 0 || e_end > h->n_ele || e_begin >= e_end) return set_err(h, BGT_EINVAL, "bad element range");
-  return track_host(h, vec6, beta, state, ix_ele_lost, nullptr, variant, n, 0, 1, e_begin, e_end);
+  return track_host(h, vec6, beta, t, state, ix_ele_lost, nullptr, variant, n, 0, 1, e_begin, e_end);
 }
 
 }  // extern "C"
@@ -716,6 +743,7 @@ struct DAArgs {
   int32_t* ixe;
   int32_t* ixt;
   int32_t* slot;
+  uint64_t* t;  // particle times (absolute time tracking) or nullptr
 };
 
 // particle index p = ((v*n_delta + d)*n_angle + a)*n_radius + r
@@ -743,6 +771,13 @@ __global__ void da_init_kernel(DAArgs A, int64_t n) {
   A.state[i] = ALIVE;
   A.ixe[i] = -1;
   A.ixt[i] = -1;
+  if (A.t) {
+    // init_coord.f90:222: t = ref_time - z / (beta c_light), ref_time = 0
+    // at the scan's starting element
+    const qp::Q t0 = qp::from_double(0.0 - A.vec6[4 * A.stride + i] / (A.beta[i] * C_LIGHT));
+    A.t[2 * i] = t0.lo;
+    A.t[2 * i + 1] = t0.hi;
+  }
   // slot of this particle: variant-major, padded per variant; inside a
   // variant radius-major ((d * n_radius + r) * n_angle + a), so that a warp
   // (and a CTA) holds probes of one or few radii across the angles -- they
@@ -829,7 +864,8 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
   CallCtx* c = L.c;
   cudaStream_t st = c->st;
   CU(h, L.use(st));
-  if ((rc = ensure_staging(h, c, n, n_slots, n_tiles))) return rc;
+  const bool with_t = h->G.abs_time != 0;
+  if ((rc = ensure_staging(h, c, n, n_slots, n_tiles, with_t))) return rc;
   int32_t* d_state = c->d_i32;
   int32_t* d_ixe = d_state + c->cap;
   int32_t* d_ixt = d_ixe + c->cap;
@@ -874,12 +910,13 @@ int bgt_da_scan_grid(bgt_handle* h, const double* ref_orbit, int32_t n_variants_
   A.ixe = d_ixe;
   A.ixt = d_ixt;
   A.slot = d_slot;
+  A.t = with_t ? c->d_t : nullptr;
   A.block = block;
   da_init_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A, n);
   da_tile_var_kernel<<<(unsigned)((n_tiles + 255) / 256), 256, 0, st>>>(d_tvar, tiles_per_var, n_tiles);
   h->launches += 2;
-  rc = track_device_impl(h, tun, c, nullptr, c->d_vec6, c->cap, c->d_beta, d_state, d_ixe, d_ixt, d_slot, d_tvar, n,
-                         n_slots, 0, n_turns, 0, h->n_ele, st);
+  rc = track_device_impl(h, tun, c, nullptr, c->d_vec6, c->cap, c->d_beta, A.t, d_state, d_ixe, d_ixt, d_slot,
+                         d_tvar, n, n_slots, 0, n_turns, 0, h->n_ele, st);
   if (rc) return rc;
   da_reduce_kernel<<<(unsigned)((n_rays + 127) / 128), 128, 0, st>>>(d_state, d_ixt, n_rays, n_radius, A.dr, 0,
                                                                      n_turns, d_da, d_surv);
@@ -986,6 +1023,9 @@ extern "C" int bgt_track_turns_device_noalloc(const bgt_element* eles, int32_t n
   if (t.compact_every < 0 || t.turns_per_launch < 0 || t.wait_limit_us < 0 ||
       (t.test_skip_table_copy != 0 && t.test_skip_table_copy != 1))
     return fail(BGT_EINVAL, "bgt_track_turns_device_noalloc: invalid tuning value");
+  if (species->absolute_time_tracking)
+    return fail(BGT_EUNSUPPORTED, "bgt_track_turns_device_noalloc: absolute time tracking needs the particle times, "
+                                  "which only the handle entry points carry");
   if (n == 0 || n_turns == 0) return 0;
   DeviceGuard dg(device);
   cudaError_t ce = dg.err;

@@ -19,7 +19,8 @@
 !                             include file bgt_track_many_gpu_case.inc)
 !   bgt_ring_free          -- release the handle
 !
-! Elements and particles are passed in Bmad's own units and integer codes;
+! Elements and particles are passed in Bmad's own units and integer codes
+! (coord_struct%t as the real(qp) array the library's time argument takes);
 ! multipole arrays come from Bmad's multipole_ele_to_ab / multipole_ele_to_kt,
 ! so the library sees exactly what track1 would use.  Particle loss is a
 ! state (coord_struct%state), not an error; err_flag is set only when the
@@ -59,6 +60,7 @@ type, bind(c) :: bgt_element_c
   real(c_double) :: fq1, fq2
   real(c_double) :: px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center
   real(c_double) :: z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center
+  real(c_double) :: delta_ref_time, ref_time_start
 end type
 
 ! bgt_species (bgt.h): the tracked species and the bmad_com switches used.
@@ -66,6 +68,7 @@ type, bind(c) :: bgt_species_c
   real(c_double) :: mass
   integer(c_int32_t) :: charge, aperture_limit_on
   real(c_double) :: max_aperture_limit
+  integer(c_int32_t) :: absolute_time_tracking, absolute_time_ref_shift
 end type
 
 ! bgt_tuning (bgt.h); all zero = the library's defaults.
@@ -95,20 +98,22 @@ interface
     type(c_ptr), value :: h
     type(bgt_tuning_c) :: t
   end function
-  integer(c_int) function bgt_track_turns(h, vec6, beta, state, ix_ele_lost, ix_turn_lost, variant, n, &
+  integer(c_int) function bgt_track_turns(h, vec6, beta, t, state, ix_ele_lost, ix_turn_lost, variant, n, &
                                           turn0, n_turns) bind(c, name='bgt_track_turns')
     import
     type(c_ptr), value :: h, variant
     real(c_double) :: vec6(*), beta(*)
+    real(qp) :: t(*)
     integer(c_int32_t) :: state(*), ix_ele_lost(*), ix_turn_lost(*)
     integer(c_int64_t), value :: n
     integer(c_int32_t), value :: turn0, n_turns
   end function
-  integer(c_int) function bgt_track_elements(h, vec6, beta, state, ix_ele_lost, variant, n, e_begin, e_end) &
+  integer(c_int) function bgt_track_elements(h, vec6, beta, t, state, ix_ele_lost, variant, n, e_begin, e_end) &
                                              bind(c, name='bgt_track_elements')
     import
     type(c_ptr), value :: h, variant
     real(c_double) :: vec6(*), beta(*)
+    real(qp) :: t(*)
     integer(c_int32_t) :: state(*), ix_ele_lost(*)
     integer(c_int64_t), value :: n
     integer(c_int32_t), value :: e_begin, e_end
@@ -246,6 +251,8 @@ do k = 1, branch%n_ele_track
   eles(k)%z_aperture_center = ele%value(z_aperture_center$)
   eles(k)%pz_aperture_width2 = ele%value(pz_aperture_width2$)
   eles(k)%pz_aperture_center = ele%value(pz_aperture_center$)
+  eles(k)%delta_ref_time = ele%value(delta_ref_time$)
+  eles(k)%ref_time_start = ele%value(ref_time_start$)
   eles(k)%an = 0;  eles(k)%bn = 0;  eles(k)%an_elec = 0;  eles(k)%bn_elec = 0
   eles(k)%knl = 0;  eles(k)%tn = 0
   if (ele%key == multipole$ .or. ele%key == ab_multipole$) then
@@ -292,6 +299,8 @@ sp%mass = mass_of(branch%param%particle)
 sp%charge = charge_of(branch%param%particle)
 sp%aperture_limit_on = merge(1, 0, bmad_com%aperture_limit_on)
 sp%max_aperture_limit = bmad_com%max_aperture_limit
+sp%absolute_time_tracking = merge(1, 0, bmad_com%absolute_time_tracking)
+sp%absolute_time_ref_shift = merge(1, 0, bmad_com%absolute_time_ref_shift)
 rc = bgt_create(bgt_ring_global%h, eles, int(branch%n_ele_track, c_int32_t), 1_c_int32_t, sp, 0_c_int32_t)
 if (rc /= bgt_ok$) then
   call out_io (s_error$, r_name, 'libbgt refused the lattice: ' // bgt_error_string(c_null_ptr))
@@ -336,6 +345,7 @@ integer i_turn, n_turns
 logical err_flag
 type (coord_struct), pointer :: p
 real(c_double), allocatable :: vec6(:), beta(:)
+real(qp), allocatable :: t(:)
 integer(c_int32_t), allocatable :: state(:), ix_ele_lost(:), ix_turn_lost(:)
 integer(c_int) rc
 integer n, ip, c
@@ -345,18 +355,19 @@ call bgt_ring_init (branch, ele_start%ix_ele, err_flag)
 if (err_flag) return
 n = size(bunch%particle)
 if (n == 0) return
-allocate (vec6(6*n), beta(n), state(n), ix_ele_lost(n), ix_turn_lost(n))
+allocate (vec6(6*n), beta(n), t(n), state(n), ix_ele_lost(n), ix_turn_lost(n))
 do ip = 1, n
   p => bunch%particle(ip)
   do c = 1, 6
     vec6((c-1)*n + ip) = p%vec(c)
   enddo
   beta(ip) = p%beta
+  t(ip) = p%t
   state(ip) = p%state
   ix_ele_lost(ip) = -1
   ix_turn_lost(ip) = -1
 enddo
-rc = bgt_track_turns(bgt_ring_global%h, vec6, beta, state, ix_ele_lost, ix_turn_lost, c_null_ptr, &
+rc = bgt_track_turns(bgt_ring_global%h, vec6, beta, t, state, ix_ele_lost, ix_turn_lost, c_null_ptr, &
                      int(n, c_int64_t), int(i_turn, c_int32_t), int(n_turns, c_int32_t))
 if (rc /= bgt_ok$) then
   call out_io (s_error$, r_name, 'libbgt: ' // bgt_error_string(bgt_ring_global%h))
@@ -370,6 +381,7 @@ do ip = 1, n
     p%vec(c) = vec6((c-1)*n + ip)
   enddo
   p%beta = beta(ip)
+  p%t = t(ip)
   p%state = state(ip)
   if (p%state /= alive$) p%ix_ele = ix_ele_lost(ip)
 enddo
@@ -390,6 +402,7 @@ type (ele_struct) ele_start
 type (coord_struct) orb
 logical err_flag
 real(c_double) vec6(6), beta(1)
+real(qp) t(1)
 integer(c_int32_t) state(1), ix_ele_lost(1), ix_turn_lost(1)
 integer(c_int) rc
 character(*), parameter :: r_name = 'bgt_track_one_turn'
@@ -399,10 +412,11 @@ if (err_flag) return
 if (orb%state /= alive$) return
 vec6 = orb%vec
 beta(1) = orb%beta
+t(1) = orb%t
 state(1) = orb%state
 ix_ele_lost(1) = -1
 ix_turn_lost(1) = -1
-rc = bgt_track_turns(bgt_ring_global%h, vec6, beta, state, ix_ele_lost, ix_turn_lost, c_null_ptr, &
+rc = bgt_track_turns(bgt_ring_global%h, vec6, beta, t, state, ix_ele_lost, ix_turn_lost, c_null_ptr, &
                      1_c_int64_t, 0_c_int32_t, 1_c_int32_t)
 if (rc /= bgt_ok$) then
   call out_io (s_error$, r_name, 'libbgt: ' // bgt_error_string(bgt_ring_global%h))
@@ -411,6 +425,7 @@ if (rc /= bgt_ok$) then
 endif
 orb%vec = vec6
 orb%beta = beta(1)
+orb%t = t(1)
 orb%state = state(1)
 if (orb%state /= alive$) orb%ix_ele = ix_ele_lost(1)
 end subroutine bgt_track_one_turn

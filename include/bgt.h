@@ -57,7 +57,7 @@
  * concurrently with other calls on the same handle.
  *
  * Scope: forward tracking (direction = time_dir = orientation = +1), relative
- * RF time (bmad_com%absolute_time_tracking = F), magnetic and electric
+ * or absolute RF time (bmad_com%absolute_time_tracking), magnetic and electric
  * multipoles (electric ones on quadrupoles, sextupoles, octupoles, thick
  * multipoles and bends), misaligned elements including bends, the bend
  * edges of every fringe type (the exact PTC edge of fringe_type full
@@ -153,6 +153,11 @@ typedef struct bgt_element {
    * (check_aperture_limit.f90:98-135); width2 = 0: no limit */
   double px_aperture_width2, px_aperture_center, py_aperture_width2, py_aperture_center;
   double z_aperture_width2, z_aperture_center, pz_aperture_width2, pz_aperture_center;
+  /* reference time through the element and at its entrance
+   * (ele%value(delta_ref_time$), ele%value(ref_time_start$), set by
+   * lat_compute_reference_energy.f90): the particle time's per-element step
+   * and, with absolute time tracking, the origin of the RF phase */
+  double delta_ref_time, ref_time_start;
 } bgt_element;
 
 /* Tracked species (lat%param%particle) and bmad_com switches. */
@@ -161,6 +166,9 @@ typedef struct bgt_species {
   int32_t charge;            /* charge_of(species) [e] */
   int32_t aperture_limit_on; /* bmad_com%aperture_limit_on (default 1) */
   double max_aperture_limit; /* bmad_com%max_aperture_limit (default 1e3 m) */
+  int32_t absolute_time_tracking;  /* bmad_com%absolute_time_tracking (default 0): the RF phase
+                                      from the particle time t instead of -z / (beta c) */
+  int32_t absolute_time_ref_shift; /* bmad_com%absolute_time_ref_shift (default 1) */
 } bgt_species;
 
 /* Launch tiles chosen by the autotuner (0 = let the library choose). */
@@ -206,21 +214,31 @@ int bgt_get_tuning(const bgt_handle* h, bgt_tuning* t);
  * state/ix_ele_lost/ix_turn_lost[n] (int32).  variant[n] selects each
  * particle's lattice variant (NULL = variant 0).  Particles whose state is
  * not alive are left untouched.  Copies in, tracks, copies out.
+ *
+ * t (may be NULL) is the particle time coord_struct%t: n IEEE binary128
+ * values (16 bytes each: a Fortran real(qp) array or C __float128[n]),
+ * advanced in every element in binary128 arithmetic exactly as the
+ * reference advances it (track_a_drift.f90:79-80,
+ * track_a_quadrupole.f90:144, track_a_bend.f90:327,
+ * track_a_thick_multipole.f90:133).  It is required with absolute time
+ * tracking, where the RF phase comes from it (particle_rf_time.f90:74-76).
+ * Tracking time runs the RARE kernel instances.
  */
-int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+int bgt_track_turns(bgt_handle* h, double* vec6, double* beta, void* t, int32_t* state, int32_t* ix_ele_lost,
                     int32_t* ix_turn_lost, const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns);
 
 /*
  * Same, DEVICE buffers already resident in HBM, enqueued on `stream`
- * (a cudaStream_t, NULL = legacy default stream).  Asynchronous: a staging
- * timeout on the device is reported by bgt_device_status.
+ * (a cudaStream_t, NULL = legacy default stream); d_t as t above, in device
+ * memory.  Asynchronous: a staging timeout on the device is reported by
+ * bgt_device_status.
  * Uses library-owned scratch sized on first use (grown as needed).
  * d_variant (device int32[n], may be NULL = variant 0) must be sorted
  * (non-decreasing); with it and more than one variant the call counts the
  * particles per variant on the device and synchronises `stream` once to read
  * the counts back (BGT_EINVAL for unsorted or out-of-range ids).
  */
-int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, int32_t* d_state,
+int bgt_track_turns_device(bgt_handle* h, double* d_vec6, double* d_beta, void* d_t, int32_t* d_state,
                            int32_t* d_ix_ele_lost, int32_t* d_ix_turn_lost, const int32_t* d_variant, int64_t n,
                            int32_t turn0, int32_t n_turns, void* stream);
 
@@ -235,10 +253,11 @@ int bgt_device_status(bgt_handle* h, void* stream);
 
 /*
  * Track n particles through table elements [e_begin, e_end) of their variant
- * once (no turn wrap), HOST buffers.  e_end - e_begin == 1 is track1
+ * once (no turn wrap), HOST buffers (t as for bgt_track_turns).
+ * e_end - e_begin == 1 is track1
  * (bmad/code/track1.f90:43) including its two check_aperture_limit calls.
  */
-int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+int bgt_track_elements(bgt_handle* h, double* vec6, double* beta, void* t, int32_t* state, int32_t* ix_ele_lost,
                        const int32_t* variant, int64_t n, int32_t e_begin, int32_t e_end);
 
 /*
@@ -281,7 +300,9 @@ int64_t bgt_kernel_launch_count(const bgt_handle* h);
  * reuses the same array and leaves its contents behind, so calls that
  * overlap on the GPU (other streams or threads) race: serialise them.  The
  * first call on a device looks up the array's address and uploads constant
- * tables; make it before any stream capture.  tuning may be NULL; otherwise
+ * tables; make it before any stream capture.  It carries no particle
+ * times, so a species with absolute time tracking is refused
+ * (BGT_EUNSUPPORTED).  tuning may be NULL; otherwise
  * (threads, CTAs per SM) must be (128, 4) or (256, 2), checked before
  * anything is enqueued (table_mode is ignored).  d_status (device int32, may
  * be NULL) receives, in stream order, the call's error flag: 1 when a

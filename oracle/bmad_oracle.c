@@ -832,8 +832,24 @@ static void track_a_drift(bgo_coord* orb, double length, int include_ref_motion,
       FL(2);
     }
   }
+  /* dt = rel_z_vel * length / (beta * ps_rel * c_light); orb%t = orb%t + dt
+   * (track_a_drift.f90:79-80): a real(rp) step added to the real(qp) time
+   * (time bookkeeping, not counted in the FP64 operation tally) */
+  if (orb->beta > 0) {
+    double dt = length / (orb->beta * ps_rel * C_LIGHT);
+    orb->t = orb->t + (__float128)dt;
+  }
   orb->vec[4] = orb->vec[4] + dz;
   FL(1);
+}
+
+/* orbit%t = start_orb%t + direction * time_dir * delta_ref_time +
+ * (start_orb%vec(5) - orbit%vec(5)) / (orbit%beta * c_light), summed left to
+ * right in real(qp) (track_a_quadrupole.f90:144, track_a_bend.f90:327,
+ * track_a_thick_multipole.f90:133). */
+static void element_exit_time(bgo_coord* orbit, const bgo_ele* ele, __float128 t0, double z0) {
+  double dz_t = (z0 - orbit->vec[4]) / (orbit->beta * C_LIGHT);
+  orbit->t = t0 + (__float128)(1 * ele->delta_ref_time) + (__float128)dz_t;
 }
 
 /* tilt_coords, bmad/code/tilt_coords.f90:18-53 */
@@ -1932,6 +1948,8 @@ static double low_energy_z_correction(const bgo_coord* orbit, const bgo_ele* ele
 /* track_a_quadrupole, bmad/low_level/track_a_quadrupole.f90:17-148 */
 static int track_a_quadrupole(bgo_coord* orbit, const bgo_ele* ele, const bgo_param* param) {
   double an[BGO_N_POLE], bn[BGO_N_POLE], ae[BGO_N_POLE], be[BGO_N_POLE], b1;
+  const __float128 t0 = orbit->t; /* start_orb = orbit (:40) */
+  const double z0 = orbit->vec[4];
   double charge_dir = 1.0;
   double length = 1 * ele->l;
   int ix_mag_max = bgo_multipole_ele_to_ab(ele, 0, 0, 1, an, bn, &b1);
@@ -1986,6 +2004,7 @@ static int track_a_quadrupole(bgo_coord* orbit, const bgo_ele* ele, const bgo_pa
     if (orbit->state != BGO_ALIVE) return 0;
   }
   if (ele->has_misalign) offset_particle(ele, 0, orbit, 1, 0, 0, 0, param);
+  element_exit_time(orbit, ele, t0, z0);
   return 0;
 }
 
@@ -1993,6 +2012,8 @@ static int track_a_quadrupole(bgo_coord* orbit, const bgo_ele* ele, const bgo_pa
  * (no elseparator / ac_kicker forms). */
 static int track_a_thick_multipole(bgo_coord* orbit, const bgo_ele* ele, const bgo_param* param) {
   double an[BGO_N_POLE], bn[BGO_N_POLE], ae[BGO_N_POLE], be[BGO_N_POLE];
+  const __float128 t0 = orbit->t; /* start_orb = orbit (:41) */
+  const double z0 = orbit->vec[4];
   double length = ele->l * 1;
   int ix_mag_max = bgo_multipole_ele_to_ab(ele, 0, 0, 1, an, bn, NULL);
   int ix_elec_max = bgo_multipole_ele_to_ab(ele, 0, 1, 0, ae, be, NULL);
@@ -2030,6 +2051,7 @@ static int track_a_thick_multipole(bgo_coord* orbit, const bgo_ele* ele, const b
     if (orbit->state != BGO_ALIVE) return 0;
   }
   if (ele->has_misalign) offset_particle(ele, 0, orbit, 1, 0, 0, 0, param);
+  element_exit_time(orbit, ele, t0, z0);
   return 0;
 }
 
@@ -2166,6 +2188,8 @@ static void bend_apply_multipole_kicks(double coef, double step_len, double r_st
 /* track_a_bend, bmad/low_level/track_a_bend.f90:18-333 */
 static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) {
   double an[BGO_N_POLE], bn[BGO_N_POLE], ae[BGO_N_POLE], be[BGO_N_POLE], b1;
+  const __float128 t0 = orbit->t; /* start_orb = orbit (:42) */
+  const double z0 = orbit->vec[4];
   if (ele->has_misalign) offset_particle(ele, 1, orbit, 1, 0, 0, 0, param);
   double rel_charge_dir = 1.0;
   int ix_elec_max = bgo_multipole_ele_to_ab(ele, 0, 1, 0, ae, be, NULL);
@@ -2289,6 +2313,7 @@ static int track_a_bend(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) 
   if (bgo_orbit_too_large(orbit, param)) return 0;
   if (apply_element_edge_kick(orbit, ele, 0, param, ae, be, ix_elec_max)) return -1;
   if (ele->has_misalign) offset_particle(ele, 0, orbit, 1, 0, 0, 0, param);
+  element_exit_time(orbit, ele, t0, z0);
   return 0;
 }
 
@@ -2350,13 +2375,24 @@ static int track_a_rfcavity(bgo_coord* orbit, const bgo_ele* ele, const bgo_para
 
   double voltage = (ele->is_on ? ele->voltage * 1 : 0.0) * charge_dir;
   double f = ele->rf_frequency;
-  /* particle_rf_time: time = -z / (beta * c_light) in real(rp), then modulo2 in real(qp) */
-  double time_dp = -orbit->vec[4] / (orbit->beta * C_LIGHT);
-  __float128 time = (__float128)time_dp;
+  /* particle_rf_time (particle_rf_time.f90:74-90): with absolute time
+   * tracking the particle time t less ref_time_start (absolute_time_ref_shift),
+   * else the relative time -z / (beta * c_light) in real(rp); then modulo2
+   * in real(qp) (:116-118).  rf_ref_time_offset is 0 for an element that is
+   * not a slave (rf_ref_time_offset.f90:30-43). */
+  __float128 time;
+  if (param->absolute_time_tracking) {
+    time = orbit->t;
+    if (param->absolute_time_ref_shift) time = time - (__float128)ele->ref_time_start;
+  } else {
+    double time_dp = -orbit->vec[4] / (orbit->beta * C_LIGHT);
+    time = (__float128)time_dp;
+  }
   if (f != 0) time = modulo2_qp(time, ((__float128)0.5) / (__float128)f);
   __float128 ph = (__float128)TWOPI * ((__float128)ele->phi0 - (time - (__float128)0.0) * (__float128)f);
   double phase0 = (double)ph;
-  phase0 = phase0 + TWOPI * ele->phi0_multipass;
+  /* no phi0_multipass with absolute time (track_a_rfcavity.f90:81) */
+  if (!param->absolute_time_tracking) phase0 = phase0 + TWOPI * ele->phi0_multipass;
   double phase = modulo2_dp(phase0, PI);
   LM(0);
   FL(8);
@@ -2401,7 +2437,10 @@ static int track1_bmad(bgo_coord* orbit, const bgo_ele* ele, bgo_param* param) {
     }
   }
   switch (key) {
-    case -1: case BGO_MARKER:
+    case -1:
+      return 0;
+    case BGO_MARKER: /* track1_bmad.f90:123-125 */
+      orbit->t = orbit->t + (__float128)ele->delta_ref_time;
       return 0;
     case BGO_RCOLLIMATOR: case BGO_ECOLLIMATOR: case BGO_MONITOR: case BGO_INSTRUMENT: case BGO_PIPE:
     case BGO_KICKER: case BGO_HKICKER: case BGO_VKICKER: case BGO_OCTUPOLE: case BGO_THICK_MULTIPOLE:
@@ -2441,6 +2480,8 @@ void bgo_init_coord(bgo_coord* orb, const double vec[6], double p0c, const bgo_p
   double pc = (1 + vec[5]) * p0c;
   orb->beta = pc / sqrt(pc * pc + param->mass * param->mass);
   orb->state = BGO_ALIVE;
+  /* init_coord.f90:222 with ref_time = 0 */
+  orb->t = (__float128)(0.0 - orb->vec[4] / (orb->beta * C_LIGHT));
 }
 
 /* track1, bmad/code/track1.f90:43-342 (no hooks, radiation, spin). */
@@ -2464,12 +2505,14 @@ void bgo_track1(bgo_coord* orb, const bgo_ele* ele, bgo_param* param) {
 /* element: bmad/multiparticle/beam_utils.f90:69-74.                     */
 
 static void track_one_particle(const bgo_ele* eles, int n_ele, bgo_param* p, double p0c, double* vec6, double* beta,
-                               int* state, int* ixe, int* ixt, long n, long i, int turn0, int n_turns) {
+                               __float128* tt, int* state, int* ixe, int* ixt, long n, long i, int turn0,
+                               int n_turns) {
   bgo_coord orb;
   for (int c = 0; c < 6; c++) orb.vec[c] = vec6[c * n + i];
   orb.beta = beta[i];
   orb.p0c = p0c;
   orb.state = state[i];
+  orb.t = tt ? tt[i] : 0;
   if (orb.state != BGO_ALIVE) return;
   for (int t = turn0; t < turn0 + n_turns && orb.state == BGO_ALIVE; t++) {
     for (int e = 0; e < n_ele; e++) {
@@ -2484,11 +2527,12 @@ static void track_one_particle(const bgo_ele* eles, int n_ele, bgo_param* p, dou
   for (int c = 0; c < 6; c++) vec6[c * n + i] = orb.vec[c];
   beta[i] = orb.beta;
   state[i] = orb.state;
+  if (tt) tt[i] = orb.t;
 }
 
 void bgo_track_turns(const bgo_ele* eles, int n_ele, const bgo_param* param, double p0c, double* vec6,
-                     double* beta, int* state, int* ix_ele_lost, int* ix_turn_lost, long n, int turn0,
-                     int n_turns, int n_threads, int element_outer) {
+                     double* beta, __float128* tq, int* state, int* ix_ele_lost, int* ix_turn_lost, long n,
+                     int turn0, int n_turns, int n_threads, int element_outer) {
   c_multi_init();
 #ifdef _OPENMP
   if (n_threads > 0) omp_set_num_threads(n_threads);
@@ -2499,7 +2543,8 @@ void bgo_track_turns(const bgo_ele* eles, int n_ele, const bgo_param* param, dou
 #pragma omp parallel for schedule(dynamic, 64)
     for (long i = 0; i < n; i++) {
       bgo_param p = *param;
-      track_one_particle(eles, n_ele, &p, p0c, vec6, beta, state, ix_ele_lost, ix_turn_lost, n, i, turn0, n_turns);
+      track_one_particle(eles, n_ele, &p, p0c, vec6, beta, tq, state, ix_ele_lost, ix_turn_lost, n, i, turn0,
+                         n_turns);
     }
     return;
   }
@@ -2515,10 +2560,12 @@ void bgo_track_turns(const bgo_ele* eles, int n_ele, const bgo_param* param, dou
         orb.beta = beta[i];
         orb.p0c = p0c;
         orb.state = state[i];
+        orb.t = tq ? tq[i] : 0;
         bgo_track1(&orb, &eles[e], &p);
         for (int c = 0; c < 6; c++) vec6[c * n + i] = orb.vec[c];
         beta[i] = orb.beta;
         state[i] = orb.state;
+        if (tq) tq[i] = orb.t;
         if (orb.state != BGO_ALIVE) {
           ix_ele_lost[i] = eles[e].ix_ele;
           ix_turn_lost[i] = t;

@@ -95,6 +95,8 @@ typedef struct bgo_param {
   double max_aperture_limit; /* bmad_com%max_aperture_limit = 1e3, bmad_struct.f90:2297 */
   int aperture_limit_on;     /* bmad_com%aperture_limit_on, default T */
   double unstable_factor;    /* lat_param_struct%unstable_factor (output) */
+  int absolute_time_tracking;  /* bmad_com%absolute_time_tracking, default F (bmad_struct.f90:2333) */
+  int absolute_time_ref_shift; /* bmad_com%absolute_time_ref_shift, default T (bmad_struct.f90:2334) */
 } bgo_param;
 
 typedef struct bgo_coord {
@@ -102,6 +104,7 @@ typedef struct bgo_coord {
   double beta;
   double p0c;
   int state;
+  __float128 t; /* coord_struct%t: the particle time, real(qp) (bmad_struct.f90:546-574) */
 } bgo_coord;
 
 typedef struct bgo_ele {
@@ -123,6 +126,10 @@ typedef struct bgo_ele {
   double r0_mag, r0_elec;
   double coupler_strength, coupler_angle, coupler_phase;
   double fq1, fq2;
+  /* ele%value(delta_ref_time$), ele%value(ref_time_start$): the reference
+   * particle's time through the element and at its entrance
+   * (lat_compute_reference_energy.f90:540-760) */
+  double delta_ref_time, ref_time_start;
   /* For BGO_MULTIPOLE: a_pole = knl, b_pole = tn, ksl_pole = ksl (pointer_to_ele_multipole). */
   double a_pole[BGO_N_POLE], b_pole[BGO_N_POLE], ksl_pole[BGO_N_POLE];
   double a_pole_elec[BGO_N_POLE], b_pole_elec[BGO_N_POLE];
@@ -151,9 +158,10 @@ void bgo_offset_particle(const bgo_ele* ele, int set, bgo_coord* orb, int s_pos_
  * ix_ele_lost is the element's ix_ele (Bmad element index), ix_turn_lost the
  * 0-based turn index in which the loss happened (-1 while alive).
  */
+/* t (may be NULL): the particle times t[n], real(qp) like coord_struct%t. */
 void bgo_track_turns(const bgo_ele* eles, int n_ele, const bgo_param* param, double p0c, double* vec6,
-                     double* beta, int* state, int* ix_ele_lost, int* ix_turn_lost, long n, int turn0,
-                     int n_turns, int n_threads, int element_outer);
+                     double* beta, __float128* t, int* state, int* ix_ele_lost, int* ix_turn_lost, long n,
+                     int turn0, int n_turns, int n_threads, int element_outer);
 
 /* Count of FP64 operations (add/sub/mul/div/sqrt = 1, libm call = 1 each,
  * tallied separately) executed by bgo_track1 since the last reset. */

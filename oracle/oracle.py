@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import struct
 import subprocess
 from pathlib import Path
 
@@ -33,11 +34,15 @@ APT = {"rectangular": 0, "elliptical": 1, "none": 0}
 
 class Param(C.Structure):
     _fields_ = [("mass", C.c_double), ("charge", C.c_int), ("max_aperture_limit", C.c_double),
-                ("aperture_limit_on", C.c_int), ("unstable_factor", C.c_double)]
+                ("aperture_limit_on", C.c_int), ("unstable_factor", C.c_double),
+                ("absolute_time_tracking", C.c_int), ("absolute_time_ref_shift", C.c_int)]
 
 
 class Coord(C.Structure):
-    _fields_ = [("vec", C.c_double * 6), ("beta", C.c_double), ("p0c", C.c_double), ("state", C.c_int)]
+    # t is the C struct's __float128 (16 bytes, 16-byte aligned); c_longdouble
+    # has that size and alignment on x86-64 and only reserves the space here
+    _fields_ = [("vec", C.c_double * 6), ("beta", C.c_double), ("p0c", C.c_double), ("state", C.c_int),
+                ("t_qp", C.c_longdouble)]
 
 
 _INTS = ["key", "ix_ele", "is_on", "fringe_type", "fringe_at", "aperture_type", "aperture_at",
@@ -48,7 +53,7 @@ _DBLS = ["l", "k1", "k2", "k3", "g", "dg", "e1", "e2", "fint", "hgap", "fintx", 
          "y_pitch", "tilt", "ref_tilt", "roll", "hkick", "vkick", "kick", "x1_limit", "x2_limit", "y1_limit",
          "y2_limit", "px_aperture_width2", "px_aperture_center", "py_aperture_width2", "py_aperture_center",
          "z_aperture_width2", "z_aperture_center", "pz_aperture_width2", "pz_aperture_center", "r0_mag", "r0_elec",
-         "coupler_strength", "coupler_angle", "coupler_phase", "fq1", "fq2"]
+         "coupler_strength", "coupler_angle", "coupler_phase", "fq1", "fq2", "delta_ref_time", "ref_time_start"]
 
 
 class Ele(C.Structure):
@@ -79,7 +84,7 @@ def _bind(lib):
     lib.bgo_offset_particle.argtypes = [C.POINTER(Ele), C.c_int, C.POINTER(Coord), C.c_int, C.c_double,
                                         C.POINTER(Param), C.POINTER(C.c_double)]
     lib.bgo_track_turns.argtypes = [C.POINTER(Ele), C.c_int, C.POINTER(Param), C.c_double, C.POINTER(C.c_double),
-                                    C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int), C.c_long, C.c_int, C.c_int, C.c_int, C.c_int]
     lib.bgo_flop_counter_read.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.bgo_c_multi.argtypes = [C.c_int, C.c_int, C.c_int]
@@ -102,8 +107,10 @@ def load(count_flops: bool = False, variant: str = "glibc"):
     return _libs[variant]
 
 
-def make_param(mass: float, charge: int = -1, aperture_limit_on: bool = True) -> Param:
-    return Param(mass, charge, 1e3, 1 if aperture_limit_on else 0, 0.0)
+def make_param(mass: float, charge: int = -1, aperture_limit_on: bool = True, absolute_time: bool = False,
+               absolute_time_ref_shift: bool = True) -> Param:
+    return Param(mass, charge, 1e3, 1 if aperture_limit_on else 0, 0.0, 1 if absolute_time else 0,
+                 1 if absolute_time_ref_shift else 0)
 
 
 def to_ele(e, lib=None, raw_bookkeeping: bool = False) -> Ele:
@@ -164,18 +171,42 @@ def track1(ele: Ele, vec6, p0c: float, param: Param, beta=None, state: int = 1, 
     return np.array(c.vec[:]), c.beta, c.state
 
 
+def coord_time_bits(c: Coord):
+    """The binary128 bits (lo, hi) of a Coord's time t."""
+    lo, hi = struct.unpack("<QQ", C.string_at(C.addressof(c) + Coord.t_qp.offset, 16))
+    return lo, hi
+
+
+def track1_timed(ele: Ele, vec6, p0c: float, param: Param, lib=None):
+    """track1 from init_coord's start (t = 0 - z / (beta c_light)); returns
+    (vec6, beta, state, start beta, start t bits, end t bits)."""
+    lib = lib or load()
+    c = Coord()
+    v = (C.c_double * 6)(*[float(x) for x in vec6])
+    lib.bgo_init_coord(C.byref(c), v, p0c, C.byref(param))
+    beta0, t0 = c.beta, coord_time_bits(c)
+    lib.bgo_track1(C.byref(c), C.byref(ele), C.byref(param))
+    return np.array(c.vec[:]), c.beta, c.state, beta0, t0, coord_time_bits(c)
+
+
 def track_turns(eles, p0c: float, param: Param, vec6: np.ndarray, beta: np.ndarray, state: np.ndarray,
                 ix_ele_lost: np.ndarray, ix_turn_lost: np.ndarray, n_turns: int, turn0: int = 0,
-                n_threads: int = 0, element_outer: bool = False, lib=None):
-    """Multi-turn tracking in place.  vec6 is (6, n) C-contiguous float64."""
+                n_threads: int = 0, element_outer: bool = False, lib=None, t: np.ndarray = None):
+    """Multi-turn tracking in place.  vec6 is (6, n) C-contiguous float64; t
+    (optional) the particle times as binary128 bits, a C-contiguous (n, 2)
+    uint64 array (bgt.qp's layout), carried in quad precision like the
+    reference's real(qp) coord_struct%t."""
     lib = lib or load()
     n = vec6.shape[1]
     assert vec6.flags["C_CONTIGUOUS"] and vec6.dtype == np.float64
+    if t is not None:
+        assert t.shape == (n, 2) and t.flags["C_CONTIGUOUS"] and t.dtype == np.uint64
     dp = C.POINTER(C.c_double)
     ip = C.POINTER(C.c_int)
     lib.bgo_track_turns(eles, len(eles), C.byref(param), p0c, vec6.ctypes.data_as(dp), beta.ctypes.data_as(dp),
-                        state.ctypes.data_as(ip), ix_ele_lost.ctypes.data_as(ip), ix_turn_lost.ctypes.data_as(ip),
-                        n, turn0, n_turns, n_threads, 1 if element_outer else 0)
+                        t.ctypes.data if t is not None else None, state.ctypes.data_as(ip),
+                        ix_ele_lost.ctypes.data_as(ip), ix_turn_lost.ctypes.data_as(ip), n, turn0, n_turns,
+                        n_threads, 1 if element_outer else 0)
 
 
 def beta_of(p0c, pz, mass):

@@ -81,7 +81,7 @@ extern "C" {
 // 1 the RARE instance always.  ix_turn_lost may be nullptr.  Returns 0,
 // BGT_EINVAL or the table compiler's code with err filled.
 int dmh_track(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const bgt_species* sp,
-              const int32_t* variant, double* vec6, double* beta, int32_t* state, int32_t* ix_ele_lost,
+              const int32_t* variant, double* vec6, double* beta, uint64_t* t, int32_t* state, int32_t* ix_ele_lost,
               int32_t* ix_turn_lost, int64_t n, int32_t rec_begin, int32_t rec_end, int32_t turn0,
               int32_t n_turns, int32_t kernel, char* err, int32_t err_len) {
   if (!eles || !sp || n_ele <= 0 || n_variants <= 0 || rec_begin < 0 || rec_end > n_ele || rec_begin > rec_end)
@@ -102,7 +102,11 @@ int dmh_track(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const 
   G.mal = sp->max_aperture_limit;
   G.ap_on = sp->aperture_limit_on;
   G.charge = sp->charge;
-  const bool rare = T.rare || kernel == 1;
+  G.abs_time = sp->absolute_time_tracking;
+  G.abs_ref_shift = sp->absolute_time_ref_shift;
+  G.track_time = t ? 1 : 0;
+  // time tracking runs the RARE instances, as on the device
+  const bool rare = T.rare || kernel == 1 || t != nullptr;
   for (int64_t i = 0; i < n; i++) {
     const int v = variant ? variant[i] : 0;
     if (v < 0 || v >= n_variants) return BGT_EINVAL;
@@ -120,6 +124,8 @@ int dmh_track(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const 
     p.state = state[i];
     int32_t ixe = ix_ele_lost[i];
     int32_t ixt = ix_turn_lost ? ix_turn_lost[i] : -1;
+    p.t_lo = t ? t[2 * i] : 0;
+    p.t_hi = t ? t[2 * i + 1] : 0;
     if (rare)
       track_one<true>(p, ixe, ixt, tab.data(), G, rec_begin, rec_end, turn0, n_turns);
     else
@@ -132,6 +138,10 @@ int dmh_track(const bgt_element* eles, int32_t n_ele, int32_t n_variants, const 
     vec6[5 * n + i] = p.pz;
     beta[i] = p.beta;
     state[i] = p.state;
+    if (t) {
+      t[2 * i] = p.t_lo;
+      t[2 * i + 1] = p.t_hi;
+    }
     ix_ele_lost[i] = ixe;
     if (ix_turn_lost) ix_turn_lost[i] = ixt;
   }

@@ -42,6 +42,19 @@ def main(ref: Path):
             continue
         rows[name.split(":")[0]] = {"tol": tol, "values": [float(v) for v in vals], "text": vals}
     out["tracking_method"] = rows
+    # the same rows tracked with absolute time (bmad_com%absolute_time_tracking
+    # = T; tracking_method_test.f90:113-119,174-179: elements with time-varying
+    # fields only)
+    abs_rows = {}
+    for line in tm:
+        p = parse_line(line)
+        if not p:
+            continue
+        name, kind, tol, vals = p
+        head = name.split(":")[0]
+        if name.endswith(": Bmad_Standard") and head.endswith("-Abs_Time"):
+            abs_rows[head[:-len("-Abs_Time")]] = {"tol": tol, "values": [float(v) for v in vals], "text": vals}
+    out["tracking_method_abs_time"] = abs_rows
     fr = {}
     for line in (ref / "regression_tests/fringe_test/output.correct").read_text().splitlines():
         p = parse_line(line)
@@ -67,7 +80,8 @@ def main(ref: Path):
             co[p[0]] = {"tol": p[2], "values": [float(v) for v in p[3]], "text": p[3]}
     out["coord"] = co
     (HERE / "reference_golden.json").write_text(json.dumps(out, indent=1, sort_keys=True))
-    print(f"tracking_method rows: {len(rows)}, fringe rows: {len(fr)}, aperture rows: {len(ap)}, "
+    print(f"tracking_method rows: {len(rows)} (+{len(abs_rows)} in absolute time), fringe rows: {len(fr)}, "
+          f"aperture rows: {len(ap)}, "
           f"multipole rows: {len(mp)}, coord rows: {len(co)}")
 
 

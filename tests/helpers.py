@@ -301,3 +301,54 @@ def config_parity_inputs(name: str):
     lat = rings.fodo_ring(apertures=c["apertures"])
     v0 = rings.gaussian_beam(getattr(rings, c["beam"]), n=c["n"])
     return lat, v0
+
+
+def qp_fraction(lo: int, hi: int):
+    """The exact value of binary128 bits (normal values and zero)."""
+    from fractions import Fraction
+
+    lo, hi = int(lo), int(hi)
+    e = (hi >> 48) & 0x7FFF
+    frac = ((hi & ((1 << 48) - 1)) << 64) | lo
+    val = Fraction(0) if (e == 0 and frac == 0) else (1 + Fraction(frac, 1 << 112)) * Fraction(2) ** (e - 16383)
+    return -val if hi >> 63 else val
+
+
+def time_residual(z0, z1, beta0, beta1, t0_bits, t1_bits, ref_time_start, delta_ref_time):
+    """The tracking_method_test's seventh column for a forward particle
+    (tracking_method_test.f90:219-221): the change of z less c_light times the
+    change of beta * (reference time - t) through the element, evaluated from
+    the particle times' exact binary128 values (the reference evaluates it in
+    real(qp)) and rounded to double."""
+    from fractions import Fraction
+
+    ref_time = ref_time_start + delta_ref_time  # ele%ref_time, real(rp)
+    ref_time_in = ref_time - delta_ref_time
+    inner = (Fraction(beta1) * (Fraction(ref_time) - qp_fraction(*t1_bits))
+             - Fraction(beta0) * (Fraction(ref_time_in) - qp_fraction(*t0_bits)))
+    return float(Fraction(z1 - z0) - Fraction(L.C_LIGHT) * inner)
+
+
+def oracle_track_timed(lat: L.Lattice, vec6: np.ndarray, start: int, stop: int, n_turns: int = 1,
+                       variant: str = "cr", absolute_time: bool = False, threads: int = 0):
+    """oracle_track_elements carrying the particle time (quad precision in the
+    oracle) from init_coord's start, t = 0 - z / (beta c_light); returns
+    (vec6, beta, state, ix_ele_lost, ix_turn_lost, t bits (n, 2) uint64)."""
+    from bgt import qp
+    from oracle import oracle as O
+
+    lib = O.load(variant=variant)
+    sub = L.Lattice(lat.elements[start:stop], lat.species, lat.p0c, lat.e_tot)
+    eles = (O.Ele * len(sub.elements))()
+    for i, e in enumerate(sub.elements):
+        eles[i] = O.to_ele(e, lib)
+    param = O.make_param(lat.species.mass, lat.species.charge, absolute_time=absolute_time)
+    v = np.ascontiguousarray(vec6, dtype=np.float64).copy()
+    n = v.shape[1]
+    b = O.beta_of(lat.p0c, v[5], lat.species.mass)
+    t = qp.initial_time(v, b)
+    st = np.ones(n, np.int32)
+    ie = np.full(n, -1, np.int32)
+    it = np.full(n, -1, np.int32)
+    O.track_turns(eles, lat.p0c, param, v, b, st, ie, it, n_turns, n_threads=threads, lib=lib, t=t)
+    return v, b, st, ie, it, t

@@ -30,9 +30,10 @@ def test_library_loads_and_exports():
 
 
 def test_struct_layout_matches_header():
-    # bgt_element: 12 int32 + 35 doubles + 6 x 22 doubles + 4 doubles
-    assert ctypes.sizeof(_lib.BgtElement) == 12 * 4 + 35 * 8 + 6 * 22 * 8 + 4 * 8 + 8 * 8
-    assert ctypes.sizeof(_lib.BgtSpecies) == 24
+    # bgt_element: 12 int32 + 35 doubles + 6 x 22 doubles + 4 doubles + 8
+    # collimator limits + 2 reference times
+    assert ctypes.sizeof(_lib.BgtElement) == 12 * 4 + 35 * 8 + 6 * 22 * 8 + 4 * 8 + 8 * 8 + 2 * 8
+    assert ctypes.sizeof(_lib.BgtSpecies) == 32
     assert ctypes.sizeof(_lib.BgtTuning) == 28
 
 

@@ -48,14 +48,14 @@ def _build(out: Path, extra=()) -> Path:
 class HostMaps:
     """bgt_create's tables and the kernel's element maps, run on the host."""
 
-    def __init__(self, lattices, so: Path):
+    def __init__(self, lattices, so: Path, absolute_time: bool = False):
         self.lats = [lattices] if isinstance(lattices, L.Lattice) else list(lattices)
         self.lib = C.CDLL(str(so))
         f = self.lib.dmh_track
         f.restype = C.c_int
         f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-                      C.c_int32, C.c_char_p, C.c_int32]
+                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                      C.c_int32, C.c_int32, C.c_char_p, C.c_int32]
         self.lib.dmh_needs_rare.restype = C.c_int
         self.lib.dmh_needs_rare.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
         self.n_ele = len(self.lats[0].elements)
@@ -64,7 +64,7 @@ class HostMaps:
             for i, e in enumerate(lat.elements):
                 self.arr[v * self.n_ele + i] = _lib.to_bgt_element(e)
         lat0 = self.lats[0]
-        self.sp = _lib.BgtSpecies(lat0.species.mass, lat0.species.charge, 1, 1e3)
+        self.sp = _lib.BgtSpecies(lat0.species.mass, lat0.species.charge, 1, 1e3, 1 if absolute_time else 0, 1)
 
     @property
     def needs_rare(self) -> bool:
@@ -72,8 +72,8 @@ class HostMaps:
         assert rc >= 0
         return rc == 1
 
-    def make_bunch(self, v0) -> Bunch:
-        return Bunch.from_vec(v0, self.lats[0].p0c, self.lats[0].species.mass)
+    def make_bunch(self, v0, with_time: bool = False) -> Bunch:
+        return Bunch.from_vec(v0, self.lats[0].p0c, self.lats[0].species.mass, with_time=with_time)
 
     def track(self, b: Bunch, rec_begin=0, rec_end=None, turn0=0, n_turns=1, variant=None, kernel=0,
               turns=True):
@@ -82,7 +82,8 @@ class HostMaps:
         err = C.create_string_buffer(512)
         rc = self.lib.dmh_track(C.addressof(self.arr), self.n_ele, len(self.lats), C.addressof(self.sp),
                                 None if var is None else var.ctypes.data, b.vec6.ctypes.data, b.beta.ctypes.data,
-                                b.state.ctypes.data, b.ix_ele_lost.ctypes.data,
+                                None if b.t is None else b.t.ctypes.data, b.state.ctypes.data,
+                                b.ix_ele_lost.ctypes.data,
                                 b.ix_turn_lost.ctypes.data if turns else None, b.n, rec_begin, rec_end, turn0,
                                 n_turns, kernel, err, 512)
         assert rc == 0, (rc, err.value)
@@ -332,3 +333,33 @@ def test_each_element_alone_picks_a_kernel_that_handles_it(so, oracle_lib, make)
         assert lean == ["D", "BSTRAIGHT"]
     else:
         assert lean == [e.name for e in base.elements]
+
+
+def test_particle_time_and_absolute_rf_on_the_host_build(so):
+    """The particle time t (binary128 in software, bgt_qp.cuh) and the RF
+    phase from it under absolute time tracking, through the kernel's own
+    element maps built for the host: t bit for bit equal to the oracle's
+    quad-precision time and the coordinates to its correctly rounded build,
+    on every golden element (relative time, and absolute time for the RF
+    rows), both zoos with losses, and the ring with apertures over 40 turns
+    in absolute time."""
+    from helpers import oracle_track_timed
+    from test_oracle_golden import ELEMENTS, GOLD, START, make_element
+
+    cases = []
+    for name in sorted(ELEMENTS):
+        cases.append((make_element(name), np.array(START, dtype=np.float64).reshape(6, 1), 1, False, name))
+        if name in GOLD["tracking_method_abs_time"]:
+            cases.append((make_element(name), np.array(START, dtype=np.float64).reshape(6, 1), 1, True,
+                          name + " abs"))
+    cases.append((zoo_lattice(), random_particles(600, seed=41, scale=3.0), 3, False, "zoo"))
+    cases.append((rare_zoo_lattice(), random_particles(600, seed=42, scale=0.1), 3, True, "rare zoo abs"))
+    cases.append((rings.fodo_ring(apertures=True),
+                  rings.gaussian_beam(rings.BeamSpec(400, 4e-6, 2e-6, 3e-3, 2e-3, seed=43)), 40, True, "ring abs"))
+    for lat, v0, turns, abs_t, what in cases:
+        hm = HostMaps(lat, so, absolute_time=abs_t)
+        b = hm.track(hm.make_bunch(v0.copy(), with_time=True), n_turns=turns)
+        ov, ob, ost, oie, oit, ot = oracle_track_timed(lat, v0.copy(), 0, len(lat), turns, absolute_time=abs_t)
+        assert_bitwise(b, ov, ob, ost, oie, oit, what)
+        assert np.array_equal(b.t, ot), what
+    assert (ost != L.ALIVE).sum() > 0  # the ring case loses particles

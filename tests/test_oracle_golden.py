@@ -136,6 +136,43 @@ def test_tracking_method_bmad_standard(name, oracle_lib):
     check_row(name, vec, GOLD["tracking_method"][name])
 
 
+@pytest.mark.parametrize("name", sorted(ELEMENTS))
+def test_tracking_method_time_column(name, oracle_lib):
+    """The rows' seventh column checks the particle time t against z: the
+    change of z less c_light times the change of beta * (reference time - t)
+    (tracking_method_test.f90:219-221), a residual of order 1e-16 when t
+    advances as the reference advances it and of order the element length
+    when it does not.  The oracle carries t in quad precision."""
+    from helpers import time_residual
+
+    lat = make_element(name)
+    e = lat.elements[0]
+    ele = O.to_ele(e, oracle_lib)
+    param = O.make_param(L.M_ELECTRON, +1)
+    vec, beta, state, beta0, t0, t1 = O.track1_timed(ele, START, lat.p0c, param, lib=oracle_lib)
+    assert state == L.ALIVE
+    d = time_residual(START[4], vec[4], beta0, beta, t0, t1, e.v("ref_time_start"), e.v("delta_ref_time"))
+    check_row(name, list(vec) + [d], GOLD["tracking_method"][name], idx=range(7))
+
+
+@pytest.mark.parametrize("name", sorted(set(ELEMENTS) & set(GOLD["tracking_method_abs_time"])))
+def test_tracking_method_absolute_time(name, oracle_lib):
+    """The "-Abs_Time" rows: the RF cavities tracked with
+    bmad_com%absolute_time_tracking = T (tracking_method_test.f90:113-119,
+    174-179), the RF phase from the particle time t less the cavity's
+    ref_time_start (particle_rf_time.f90:74-76) folded in quad precision."""
+    from helpers import time_residual
+
+    lat = make_element(name)
+    e = lat.elements[0]
+    ele = O.to_ele(e, oracle_lib)
+    param = O.make_param(L.M_ELECTRON, +1, absolute_time=True)
+    vec, beta, state, beta0, t0, t1 = O.track1_timed(ele, START, lat.p0c, param, lib=oracle_lib)
+    assert state == L.ALIVE
+    d = time_residual(START[4], vec[4], beta0, beta, t0, t1, e.v("ref_time_start"), e.v("delta_ref_time"))
+    check_row(name + "-Abs_Time", list(vec) + [d], GOLD["tracking_method_abs_time"][name], idx=range(7))
+
+
 def test_fringe_hwang_edges(oracle_lib):
     # fringe_test.bmad: b: sbend, e1 = 0.1, e2 = -0.2, k1 = 0.1, g = 0.1, fint = 0.5, hgap = 0.4
     e = L.Element("sbend", "B", {"l": 0.0, "e1": 0.1, "e2": -0.2, "k1": 0.1, "g": 0.1, "fint": 0.5, "hgap": 0.4})

@@ -120,8 +120,8 @@ def test_null_handle_calls_return_einval():
     bp = _lib.ptr(b, C.c_double)
     sp = _lib.ptr(s, C.c_int32)
     ip = _lib.ptr(i, C.c_int32)
-    assert lib.bgt_track_turns(None, dp, bp, sp, ip, ip, None, 1, 0, 1) == _lib.BGT_EINVAL
-    assert lib.bgt_track_elements(None, dp, bp, sp, ip, None, 1, 0, 1) == _lib.BGT_EINVAL
+    assert lib.bgt_track_turns(None, dp, bp, None, sp, ip, ip, None, 1, 0, 1) == _lib.BGT_EINVAL
+    assert lib.bgt_track_elements(None, dp, bp, None, sp, ip, None, 1, 0, 1) == _lib.BGT_EINVAL
     t = _lib.BgtTuning(128, 4, 0, 0, 0)
     assert lib.bgt_set_tuning(None, C.byref(t)) == _lib.BGT_EINVAL
     assert lib.bgt_get_tuning(None, C.byref(t)) == _lib.BGT_EINVAL
@@ -145,7 +145,7 @@ def test_error_messages_are_per_thread():
     other = []
 
     def worker():
-        lib.bgt_track_elements(None, None, None, None, None, None, 1, 0, 1)
+        lib.bgt_track_elements(None, None, None, None, None, None, None, 1, 0, 1)
         other.append(lib.bgt_last_error(None))
 
     th = threading.Thread(target=worker)
