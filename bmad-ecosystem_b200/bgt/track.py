@@ -202,8 +202,8 @@ class Tracker:
                   (ix_turn_lost, torch.int32)]
         if variant is not None:
             checks.append((variant, torch.int32))
-        for t, dt in checks:
-            if not t.is_cuda or t.dtype != dt or not t.is_contiguous():
+        for x, dt in checks:
+            if not x.is_cuda or x.dtype != dt or not x.is_contiguous():
                 raise ValueError("device tensors must be contiguous CUDA tensors of the documented dtype")
         n = beta.numel()
         if vec6.numel() != 6 * n or (variant is not None and variant.numel() != n):

@@ -129,12 +129,41 @@ BGT_HD bool round_test(dd v, double err, double* out) {
 // Below 2^-27, |x|^3/6 (asin, sinh: x^3/6; atan: x^3/3) is below half an ulp
 // of x and x^2/2 below half an ulp of 1, so the correctly rounded value is
 // x (odd) or 1 (even); that also keeps every product here normal.
+//
+// The polynomials are evaluated by Estrin's scheme with fused multiply-adds
+// (independent pairs first, then powers y^2, y^4): the same terms with a
+// dependency chain of depth ~log2(K) instead of K.  Its rounding error is of
+// the Horner bound's order: every partial sum is the leading coefficient plus
+// terms smaller by y <= 2^-8, so P still carries < 2u + O(u y) relative
+// error, within the 8u of the bounds above.
+
+// C[f] + C[f+1] y + ... + C[K] y^(K-f) by Estrin's scheme (fused multiply-adds)
+template <int F, int K>
+BGT_HD double poly_estrin(double y, const double (*C)[2]) {
+  constexpr int N = K - F + 1;  // number of coefficients: 4, 5 or 8
+  static_assert(N == 4 || N == 5 || N == 8, "poly_estrin: 4, 5 or 8 coefficients");
+  const double y2 = y * y;
+  const double b0 = fma(C[F + 1][0], y, C[F][0]);
+  const double b1 = fma(C[F + 3][0], y, C[F + 2][0]);
+  if constexpr (N == 4) {
+    return fma(b1, y2, b0);
+  } else {
+    const double y4 = y2 * y2;
+    const double c0 = fma(b1, y2, b0);
+    if constexpr (N == 5) {
+      return fma(C[K][0], y4, c0);
+    } else {
+      const double b2 = fma(C[F + 5][0], y, C[F + 4][0]);
+      const double b3 = fma(C[F + 7][0], y, C[F + 6][0]);
+      return fma(fma(b3, y2, b2), y4, c0);
+    }
+  }
+}
+
 template <int K>
 BGT_HD bool odd_series_light(double x, const double (*C)[2], double* out) {
   double y = x * x;
-  double p = C[K][0];
-#pragma unroll
-  for (int k = K - 1; k >= 1; k--) p = p * y + C[k][0];
+  double p = poly_estrin<1, K>(y, C);
   double c = (x * y) * p;
   dd s = fast_two_sum(x, c);
   double err = fabs(c) * 0x1p-50 + fabs(x) * 0x1p-69;
@@ -144,9 +173,7 @@ BGT_HD bool odd_series_light(double x, const double (*C)[2], double* out) {
 template <int K>
 BGT_HD bool even_series_light(double x, const double (*C)[2], double* out) {
   dd y = two_prod(x, x);
-  double q = C[K][0];
-#pragma unroll
-  for (int k = K - 1; k >= 2; k--) q = q * y.hi + C[k][0];
+  double q = poly_estrin<2, K>(y.hi, C);
   double t = (y.hi * y.hi) * q;
   dd s = fast_two_sum(1.0, y.hi * C[1][0]);
   s.lo = s.lo + (y.lo * C[1][0] + t);
@@ -486,9 +513,7 @@ BGT_HD double atan2(double y, double x) {
     // odd-series bound for atan(qh) (K = 8) plus the rounding of c + ql,
     // the error of ql (u) and the dropped ql qh^2 term (< 2 |ql| yy).
     double yy = qh * qh;
-    double p = ATAN_C[8][0];
-#pragma unroll
-    for (int k = 7; k >= 1; k--) p = p * yy + ATAN_C[k][0];
+    double p = poly_estrin<1, 8>(yy, ATAN_C);
     double c = (qh * yy) * p;
     double t = c + ql;
     dd s = fast_two_sum(qh, t);

@@ -373,35 +373,49 @@ __device__ __forceinline__ double drift_pz_term(const Part& p, const Glob& G, Dr
   return m.a;
 }
 
+// a / b correctly rounded from r = RN(1 / b): q = RN(a r) is within an ulp
+// of a / b, the remainder e = a - b q is exact (one fused multiply-add), and
+// RN(q + e r) is the correctly rounded quotient (Markstein's theorem; IEEE
+// division bit for bit).  e = 0 means q is exact already, which keeps the
+// sign of a zero quotient.  Three instructions in place of a division for
+// every further quotient by the same divisor.
+__device__ __forceinline__ double div_by(double a, double b, double r) {
+  const double q = a * r;
+  const double e = fma(-q, b, a);
+  return e == 0 ? q : fma(e, r, q);
+}
+
 template <bool REF_MOTION>
 __device__ __forceinline__ void track_a_drift(Part& p, double length, const Glob& G, DriftMemo& m) {
   if (length == 0) return;
   double rel_pc = 1 + p.pz;
-  double px_rel = p.px / rel_pc;
-  double py_rel = p.py / rel_pc;
+  const double r_pc = 1.0 / rel_pc;
+  double px_rel = div_by(p.px, rel_pc, r_pc);
+  double py_rel = div_by(p.py, rel_pc, r_pc);
   double pxy2 = px_rel * px_rel + py_rel * py_rel;
   if (pxy2 >= 1) {
     p.state = LOST_PZ;
     return;
   }
   double ps_rel = sqrt(1 - pxy2);
-  p.x = p.x + length * px_rel / ps_rel;
-  p.y = p.y + length * py_rel / ps_rel;
+  const double r_ps = 1.0 / ps_rel;
+  p.x = p.x + div_by(length * px_rel, ps_rel, r_ps);
+  p.y = p.y + div_by(length * py_rel, ps_rel, r_ps);
   double dz;
   if (p.beta > 0) {
     if (REF_MOTION) {
       double a = drift_pz_term(p, G, m);
       // sqrt_one(-pxy2) = -pxy2 / (sqrt(1 + (-pxy2)) + 1), and
       // sqrt(1 + (-pxy2)) is ps_rel bit for bit (1 + (-a) == 1 - a)
-      dz = length * (a + (-pxy2 / (ps_rel + 1.0)) / ps_rel);
+      dz = length * (a + div_by(-pxy2 / (ps_rel + 1.0), ps_rel, r_ps));
     } else {
-      dz = -length / ps_rel;
+      dz = -div_by(length, ps_rel, r_ps);
     }
   } else {
     if (REF_MOTION) {
-      dz = length * (1 - 1 / ps_rel);
+      dz = length * (1 - r_ps);
     } else {
-      dz = -length / ps_rel;
+      dz = -div_by(length, ps_rel, r_ps);
     }
   }
   // dt = rel_z_vel * length / (beta * ps_rel * c_light); t = t + dt

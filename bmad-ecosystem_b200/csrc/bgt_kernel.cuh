@@ -610,8 +610,9 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
           p.state = LOST_PZ;
           return;
         }
-        double g_p = g_tot / pt;
-        double phi_1 = cr::asin(px / pt);
+        const double r_pt = 1.0 / pt;  // the four quotients by pt from one reciprocal
+        double g_p = div_by(g_tot, pt, r_pt);
+        double phi_1 = cr::asin(div_by(px, pt, r_pt));
         double sin_plus = cr::sin(angle + phi_1), cos_plus = cr::cos(angle + phi_1);
         double gx1 = 1 + g * x;
         double t1 = gx1 * step_len * sinc_a;
@@ -640,8 +641,8 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
         double angle_p = 2 * (angle + phi_1 - 1 * cr::atan2(L_u, -L_v));
         double L_p = 1 * L_c / sinc_d(angle_p / 2);
         p.px = pt * cr::sin(phi_1 + angle - angle_p);
-        p.y = y + py * L_p / pt;
-        p.z = z + p.beta * step_len / q[B_BETAREF] - rel_p * L_p / pt;
+        p.y = y + div_by(py * L_p, pt, r_pt);
+        p.z = z + p.beta * step_len / q[B_BETAREF] - div_by(rel_p * L_p, pt, r_pt);
       }
     }
     if (ix > -1) bend_multipole_kicks(p, q, an, bn, ix, (n == n_step) ? 0.5 : 1.0, G);
