@@ -373,16 +373,27 @@ __device__ __forceinline__ double drift_pz_term(const Part& p, const Glob& G, Dr
   return m.a;
 }
 
-// a / b correctly rounded from r = RN(1 / b): q = RN(a r) is within an ulp
-// of a / b, the remainder e = a - b q is exact (one fused multiply-add), and
-// RN(q + e r) is the correctly rounded quotient (Markstein's theorem; IEEE
-// division bit for bit).  e = 0 means q is exact already, which keeps the
-// sign of a zero quotient.  Three instructions in place of a division for
-// every further quotient by the same divisor.
+// a / b correctly rounded from r = RN(1 / b), IEEE division bit for bit.
+// q0 = RN(a r) can be up to 1.5 ulp from a / b (r carries up to half an ulp
+// of 1 / b), so one Newton correction q1 = RN(q0 + (a - b q0) r) comes first:
+// it lands within 0.5 ulp plus a few 2^-52 ulp of a / b, hence within one
+// ulp.  From there Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1),
+// 1990; Muller et al., Handbook of Floating-Point Arithmetic, "Markstein's
+// theorem" in the division chapter) gives it: with r within half an ulp of
+// 1 / b and q1 within one ulp of a / b, the remainder a - b q1 is exact and
+// RN(q1 + (a - b q1) r) = RN(a / b).  A zero first remainder means q0 is
+// exact (and keeps the sign of a zero quotient).  |a| below 2^-960 goes to
+// the division, where the remainders could leave the normal range; b is a
+// momentum-like quantity here, far from overflow of r.  Five fused
+// operations in place of a division for each quotient by the same divisor.
 __device__ __forceinline__ double div_by(double a, double b, double r) {
-  const double q = a * r;
-  const double e = fma(-q, b, a);
-  return e == 0 ? q : fma(e, r, q);
+  const double q0 = a * r;
+  const double e0 = fma(-q0, b, a);
+  if (e0 == 0) return q0;
+  if (fabs(a) < 0x1p-960) return a / b;
+  const double q1 = fma(e0, r, q0);
+  const double e1 = fma(-q1, b, a);
+  return fma(e1, r, q1);
 }
 
 template <bool REF_MOTION>
