@@ -734,6 +734,7 @@ static int compile_element(const bgt_element& e, const bgt_species& sp, double p
       put_edge(q + B_EDGE, e, true);
       put_edge(q + B_EDGE + EDGE_N, e, false);
       q[B_DTREF] = e.delta_ref_time;
+      q[B_RBETAREF] = 1.0 / q[B_BETAREF];
       // bend_edge_kick (fringe_mod.f90:39-127): the Hwang map for basic_bend,
       // hard_edge_only and sad_full; the SAD soft edge for soft_edge_only and
       // sad_full (nothing when fint hgap or g + dg is zero); the linear edge;

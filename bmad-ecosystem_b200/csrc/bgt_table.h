@@ -188,7 +188,8 @@ constexpr int EDGE_GT = 0, EDGE_GT2 = 1, EDGE_GS2 = 2, EDGE_K1TANE = 3, EDGE_K1T
               EDGE_C1 = 6, EDGE_C3 = 7, EDGE_C4 = 8, EDGE_GPG = 9, EDGE_GTGS2_2K1 = 10;
 constexpr int EDGE_N = 11;
 constexpr int B_DTREF = B_EDGE + 2 * EDGE_N;  // delta_ref_time
-constexpr int B_N = B_DTREF + 1;
+constexpr int B_RBETAREF = B_DTREF + 1;       // RN(1 / beta_ref): divides by beta_ref via div_by
+constexpr int B_N = B_RBETAREF + 1;
 
 // Exact bend edge block (F_EXACT_EDGE, exact_bend_edge_kick,
 // fringe_mod.f90:1465-1686): beta0 = p0c / e_tot, 1 / beta0,

@@ -22,8 +22,10 @@ static double uni() {  // [0, 1)
   return (S >> 11) * (1.0 / 9007199254740992.0);
 }
 // uniform in [lo, hi] (mode 0) or sign * 2^uniform(log2 lo, log2 hi) (mode 1)
+// (modes 2 and 3: atan2 as mode 0, both operands then scaled by 2^-1000 /
+// 2^-1040, tiny and subnormal denominators)
 static double draw(double lo, double hi, int mode) {
-  if (mode == 0) return lo + (hi - lo) * uni();
+  if (mode != 1) return lo + (hi - lo) * uni();
   double e = std::log2(lo) + (std::log2(hi) - std::log2(lo)) * uni();
   double v = std::exp2(e);
   return (uni() < 0.5) ? -v : v;
@@ -75,7 +77,7 @@ int main(int argc, char** argv) {
       // double-double fast paths and the slow paths behind them
       {"sin", -0.78, 0.78, 0}, {"sin", -30.0, 30.0, 0}, {"cos", -0.78, 0.78, 0}, {"cos", -30.0, 30.0, 0},
       {"sinh", -2.0, 2.0, 0}, {"cosh", -2.0, 2.0, 0}, {"exp", -2.0, 2.0, 0}, {"asin", -1.0, 1.0, 0},
-      {"atan2", -4.0, 4.0, 0},
+      {"atan2", -4.0, 4.0, 0}, {"atan2", -0.0625, 0.0625, 2}, {"atan2", -4.0, 4.0, 3},
       {"tan", 0x1p-30, 0x1p-4, 1}, {"tan", -1.5, 1.5, 0}, {"tan", -30.0, 30.0, 0},
       {"atan", 0x1p-30, 0x1p-4, 1}, {"atan", -4.0, 4.0, 0}, {"atan", -1e3, 1e3, 0},
   };
@@ -89,6 +91,13 @@ int main(int argc, char** argv) {
         double den = (i % 8 == 7) ? -(0.25 + 2 * uni()) : (0.25 + 2 * uni());
         y = x * den;
         x = den;
+        if (r.mode == 2) {
+          x *= 0x1p-1000;
+          y *= 0x1p-1000;
+        } else if (r.mode == 3) {
+          x *= 0x1p-1040;
+          y *= 0x1p-1040;
+        }
       }
       double c = cr_eval(r.fn, x, y), q = q_eval(r.fn, x, y);
       if (c != q && !(std::isnan(c) && std::isnan(q))) {
