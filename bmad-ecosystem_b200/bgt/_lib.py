@@ -63,7 +63,7 @@ EXPORTED = [
     # include/bgt_mlp.h
     "bgt_mlp_create", "bgt_mlp_destroy", "bgt_mlp_last_error", "bgt_mlp_launch_count", "bgt_mlp_get_params",
     "bgt_mlp_set_params", "bgt_mlp_forward", "bgt_mlp_gradients", "bgt_mlp_train_step", "bgt_mlp_features",
-    "bgt_mlp_gemm_bf16",
+    "bgt_mlp_gemm_bf16", "bgt_mlp_gemm_bf16_wait_test",
 ]
 
 _dp = C.POINTER(C.c_double)

@@ -47,6 +47,7 @@ def _bind():
     lib.bgt_mlp_train_step.argtypes = [vp, vp, vp, i32, C.c_float, f32p, vp]
     lib.bgt_mlp_features.argtypes = [vp, vp, i64, i64, vp, vp, i32, vp, vp, vp, vp, vp]
     lib.bgt_mlp_gemm_bf16.argtypes = [vp, i64, vp, i64, i32, i32, i32, vp, vp]
+    lib.bgt_mlp_gemm_bf16_wait_test.argtypes = [vp, i64, vp, i64, i32, i32, i32, vp, C.c_uint32, vp]
     _mlp_bound = True
     return lib
 
@@ -79,6 +80,21 @@ def gemm_bf16(a, b):
     if rc != 0:
         raise _lib.BgtError(f"bgt_mlp_gemm_bf16 failed ({rc})")
     return c
+
+
+def gemm_wait_test(a, b, wait_limit_us: int = 1000) -> int:
+    """Return code of the GEMM launched with no MMA issued (its bounded
+    mbarrier waits run out after wait_limit_us); BGT_ETIMEOUT expected."""
+    import torch
+
+    lib = _bind()
+    _need(a, torch.bfloat16, "a")
+    _need(b, torch.bfloat16, "b")
+    m, k = a.shape
+    n = b.shape[0]
+    c = torch.empty((m, n), dtype=torch.float32, device=a.device)
+    return int(lib.bgt_mlp_gemm_bf16_wait_test(a.data_ptr(), k, b.data_ptr(), b.shape[1], m, n, k, c.data_ptr(),
+                                               wait_limit_us, _stream(a)))
 
 
 def pad_rows(n: int) -> int:

@@ -97,12 +97,12 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
   return t;
 }
-// Wait for the phase of `parity` to complete; false after 2 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Wait for the phase of `parity` to complete; false after limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
   return true;
 }
@@ -194,7 +194,7 @@ __device__ int g_gemm_error;
 template <int NT, int EPI>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_kernel(const bf16* __restrict__ A, int64_t lda, const bf16* __restrict__ B, int64_t ldb, int k_blocks,
-                Epi ep, int* err) {
+                Epi ep, int* err, uint64_t wait_ns, int skip_mma) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ uint32_t tmem_slot;
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (kb >= 1) {
         // the MMAs of block kb-1 read stage s1: wait before refilling it
         // (the outcome is made CTA-uniform before anyone leaves the loop)
-        const bool w = mbar_wait(s1 ? bar1 : bar0, ((kb - 1) >> 1) & 1);
+        const bool w = mbar_wait(s1 ? bar1 : bar0, ((kb - 1) >> 1) & 1, wait_ns);
         if (!__syncthreads_and(w)) {
           ok = false;
           break;
@@ -248,7 +248,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     fence_proxy_async();
     __syncthreads();
-    if (tid == 0) {
+    // skip_mma (tests only): no MMA and no commit are issued, so the
+    // mbarrier waits run out with nothing outstanding
+    if (tid == 0 && !skip_mma) {
       tc_fence_after();
       const uint32_t a_s = s ? sA1 : sA0, b_s = s ? sB1 : sB0;
 #pragma unroll
@@ -262,12 +264,12 @@ __global__ void __launch_bounds__(THREADS, 1)
   cp_async_wait<0>();
   const int last = k_blocks - 1;
   const uint32_t last_bar = (last & 1) ? bar1 : bar0;
-  if (ok) ok = mbar_wait(last_bar, (last >> 1) & 1);
+  if (ok) ok = mbar_wait(last_bar, (last >> 1) & 1, wait_ns);
   ok = __syncthreads_and(ok);  // tcgen05.ld below is warp-collective
   if (!ok) {
     atomicExch(err, 1);
     // bounded second wait for the MMAs in flight before tensor memory is freed
-    mbar_wait(last_bar, (last >> 1) & 1);
+    mbar_wait(last_bar, (last >> 1) & 1, wait_ns);
   }
   tc_fence_after();
   __syncwarp();
@@ -326,7 +328,8 @@ constexpr int gemm_smem() {
 
 template <int NT, int EPI>
 static cudaError_t launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int m_tiles, int splits,
-                               int k_blocks, const Epi& ep, int* err, cudaStream_t st) {
+                               int k_blocks, const Epi& ep, int* err, cudaStream_t st,
+                               uint64_t wait_ns = 2000000000ull, int skip_mma = 0) {
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -336,7 +339,8 @@ static cudaError_t launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_
     if (e != cudaSuccess) return e;
     attr_set[dev & 63] = true;
   }
-  gemm_kernel<NT, EPI><<<dim3(m_tiles, splits), THREADS, gemm_smem<NT>(), st>>>(A, lda, B, ldb, k_blocks, ep, err);
+  gemm_kernel<NT, EPI><<<dim3(m_tiles, splits), THREADS, gemm_smem<NT>(), st>>>(A, lda, B, ldb, k_blocks, ep, err, wait_ns,
+                                                                              skip_mma);
   return cudaGetLastError();
 }
 
@@ -805,8 +809,8 @@ int bgt_mlp_features(const double* d_vec0, const double* d_vec, int64_t n, int64
   return cudaGetLastError() == cudaSuccess ? 0 : BGT_ECUDA;
 }
 
-int bgt_mlp_gemm_bf16(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int32_t m, int32_t n,
-                      int32_t k, float* d_c, void* stream) {
+static int gemm_bf16(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int32_t m, int32_t n,
+                     int32_t k, float* d_c, void* stream, uint64_t wait_ns, int skip_mma) {
   if (!d_a || !d_b || !d_c || m <= 0 || m % BM || (n != 64 && n != 256) || k <= 0 || k % BK) return BGT_EINVAL;
   if (lda < k || ldb < k || lda % 8 || ldb % 8 || !aligned16(d_a) || !aligned16(d_b) || !aligned16(d_c))
     return BGT_EINVAL;
@@ -818,13 +822,25 @@ int bgt_mlp_gemm_bf16(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int
   e.out_f32 = d_c;
   const bf16* A = reinterpret_cast<const bf16*>(d_a);
   const bf16* B = reinterpret_cast<const bf16*>(d_b);
-  cudaError_t ce = (n == 256) ? launch_gemm<256, EPI_F32>(A, lda, B, ldb, m / BM, 1, k / BK, e, d_err, st)
-                              : launch_gemm<64, EPI_F32>(A, lda, B, ldb, m / BM, 1, k / BK, e, d_err, st);
+  cudaError_t ce = (n == 256)
+                       ? launch_gemm<256, EPI_F32>(A, lda, B, ldb, m / BM, 1, k / BK, e, d_err, st, wait_ns, skip_mma)
+                       : launch_gemm<64, EPI_F32>(A, lda, B, ldb, m / BM, 1, k / BK, e, d_err, st, wait_ns, skip_mma);
   if (ce != cudaSuccess) return BGT_ECUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return BGT_ECUDA;
   int flag = 0;
   if (cudaMemcpy(&flag, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BGT_ECUDA;
   return flag ? BGT_ETIMEOUT : 0;
+}
+
+int bgt_mlp_gemm_bf16(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int32_t m, int32_t n,
+                      int32_t k, float* d_c, void* stream) {
+  return gemm_bf16(d_a, lda, d_b, ldb, m, n, k, d_c, stream, 2000000000ull, 0);
+}
+
+int bgt_mlp_gemm_bf16_wait_test(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int32_t m,
+                                int32_t n, int32_t k, float* d_c, uint32_t wait_limit_us, void* stream) {
+  if (wait_limit_us == 0) return BGT_EINVAL;
+  return gemm_bf16(d_a, lda, d_b, ldb, m, n, k, d_c, stream, (uint64_t)wait_limit_us * 1000ull, 1);
 }
 
 }  // extern "C"

@@ -85,6 +85,13 @@ int bgt_mlp_features(const double* d_vec0, const double* d_vec, int64_t n, int64
 int bgt_mlp_gemm_bf16(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int32_t m, int32_t n,
                       int32_t k, float* d_c, void* stream);
 
+/* Test of the GEMM's bounded mbarrier waits: the same launch with no MMA and
+ * no commit issued, so every wait runs out after wait_limit_us (> 0) with
+ * nothing outstanding; the kernel frees its tensor memory and returns, and
+ * the call reports BGT_ETIMEOUT.  d_c is not written. */
+int bgt_mlp_gemm_bf16_wait_test(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int64_t ldb, int32_t m,
+                                int32_t n, int32_t k, float* d_c, uint32_t wait_limit_us, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,24 @@ def test_gemm_matches_torch(m, n, k):
     assert err < 1e-5, err
 
 
+def test_gemm_bounded_wait_reports_timeout():
+    """The GEMM launched with no MMA issued: every mbarrier wait runs out
+    after 1 ms with nothing outstanding, the kernel frees its tensor memory
+    and returns, the call reports BGT_ETIMEOUT, and the context stays usable
+    (a normal GEMM afterwards is exact)."""
+    from bgt import _lib, mlp
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(5)
+    a = torch.randn(256, 128, generator=g).to(dev).to(torch.bfloat16)
+    b = torch.randn(64, 128, generator=g).to(dev).to(torch.bfloat16)
+    assert mlp.gemm_wait_test(a, b, 1000) == _lib.BGT_ETIMEOUT
+    c = mlp.gemm_bf16(a, b)
+    ref = a.double() @ b.double().T
+    scale = a.double().abs() @ b.double().abs().T
+    assert ((c.double() - ref).abs() / scale).max().item() < 1e-5
+
+
 def _random_net(seed=3, n=1024):
     rng = np.random.default_rng(seed)
     p = M.init_params(seed=seed).astype(np.float32)
