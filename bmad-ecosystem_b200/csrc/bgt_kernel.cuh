@@ -115,10 +115,6 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
   // has identical inputs at every step, so it is evaluated once.
   QMat mx, my;
   double rel_p_m = NAN;
-  // Without electric kicks pz and beta stay fixed through the body, so the
-  // per-step low-energy z correction is the same value at every step.
-  const bool elec = RARE && ixe > -1;
-  const double dz_lez = elec ? 0.0 : low_energy_z_correction(p, q + Q_LEZ, step);
   for (int i = 1; i <= n_step; i++) {
     double rel_p = 1 + p.pz;
     if (!(rel_p == rel_p_m)) {
@@ -149,7 +145,7 @@ __device__ __forceinline__ void body_quad(Part& p, const Rec& R, const Glob& G, 
     p.px = mx.m10 * x + mx.cx * px;
     p.y = my.cx * y + my.m01 * py;
     p.py = my.m10 * y + my.cx * py;
-    p.z = p.z + (elec ? low_energy_z_correction(p, q + Q_LEZ, step) : dz_lez);
+    p.z = p.z + low_energy_z_correction(p, q + Q_LEZ, step);
     if (ix > -1) ab_multipole_kicks(p, an, bn, ix, (i == n_step) ? q[Q_RHALF] : q[Q_RSTEP]);
     if (RARE && ixe > -1) ab_multipole_kicks_elec(p, ae, be, ixe, (i == n_step) ? q[Q_STEP] / 2 : q[Q_STEP], G);
   }
@@ -586,14 +582,6 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
   if (RARE && ixe > -1) bend_elec_kicks(p, ae, be, ixe, 0.5, q[B_STEP], q[B_G], G);
   const double g = q[B_G];
   const double step_len = q[B_STEP];
-  // Without electric kicks beta and pz stay fixed through the body: the
-  // exact body's beta * step_len / beta_ref is one value for every step, and
-  // pt = sqrt(rel_p^2 - py^2) with its reciprocal and g_tot / pt change only
-  // when a multipole kick changes py (value-identical memo keyed on py and
-  // rel_p).
-  const bool elec = RARE && ixe > -1;
-  const double dz_beta = div_by(p.beta * step_len, q[B_BETAREF], q[B_RBETAREF]);
-  double pt_key_py = NAN, pt_key_rel_p = NAN, pt = 0, r_pt = 0, g_p = 0;
   for (int n = 1; n <= n_step; n++) {
     if (fl & F_K1_BODY) {
       sbend_k1_body(p, q);
@@ -617,17 +605,13 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
         const double g_tot = q[B_GTOT];
         const double angle = q[B_ANGLE];
         const double sinc_a = q[B_SINCA];
-        if (!(py == pt_key_py && rel_p == pt_key_rel_p)) {
-          pt = sqrt(rel_p2 - py * py);
-          r_pt = 1.0 / pt;  // the four quotients by pt from one reciprocal
-          g_p = div_by(g_tot, pt, r_pt);
-          pt_key_py = py;
-          pt_key_rel_p = rel_p;
-        }
+        double pt = sqrt(rel_p2 - py * py);
         if (fabs(px) > pt) {
           p.state = LOST_PZ;
           return;
         }
+        const double r_pt = 1.0 / pt;  // the four quotients by pt from one reciprocal
+        double g_p = div_by(g_tot, pt, r_pt);
         double phi_1 = cr::asin(div_by(px, pt, r_pt));
         double sin_plus = cr::sin(angle + phi_1), cos_plus = cr::cos(angle + phi_1);
         double gx1 = 1 + g * x;
@@ -658,8 +642,7 @@ __device__ __forceinline__ void body_bend(Part& p, const Rec& R, const Glob& G, 
         double L_p = 1 * L_c / sinc_d(angle_p / 2);
         p.px = pt * cr::sin(phi_1 + angle - angle_p);
         p.y = y + div_by(py * L_p, pt, r_pt);
-        p.z = z + (elec ? div_by(p.beta * step_len, q[B_BETAREF], q[B_RBETAREF]) : dz_beta) -
-              div_by(rel_p * L_p, pt, r_pt);
+        p.z = z + div_by(p.beta * step_len, q[B_BETAREF], q[B_RBETAREF]) - div_by(rel_p * L_p, pt, r_pt);
       }
     }
     if (ix > -1) bend_multipole_kicks(p, q, an, bn, ix, (n == n_step) ? 0.5 : 1.0, G);
