@@ -4,23 +4,42 @@
 // accumulators in tensor memory), the output layer / loss / Adam on CUDA
 // cores.  C ABI in include/bgt_mlp.h.  No counterpart in the reference.
 //
-// GEMM kernel (gemm_kernel<NT, EPI>): one CTA of 128 threads computes a
-// 128 x NT tile (NT = 256 or 64) of A[M][K] . B[N][K]^T, both operands
-// K-major (row-major with K contiguous).  K advances in blocks of 64 bf16
-// (128 bytes per row): each block of A (128 rows) and B (NT rows) is copied
-// into shared memory with 16-byte cp.async in the canonical 128-byte-swizzled
-// K-major layout (8-row atoms of 1024 bytes, 16-byte chunk c of row r stored
-// at chunk c ^ (r % 8)), two stages deep.  One elected thread issues four
-// tcgen05.mma (M=128, N=NT, K=16) per block and commits them to the stage's
-// mbarrier; the stage is refilled only after that mbarrier completes.  The
-// accumulator lives in NT tensor-memory columns (lane = tile row); the four
-// warps read their 32 lanes with tcgen05.ld and run the epilogue:
-//   EPI_FWD  bias + ReLU -> bf16 row-major and (optionally) transposed copies
+// GEMM kernel (gemm_kernel<NT, EPI>): C = A[M][K] . B[NT][K]^T with both
+// operands K-major (row-major, K contiguous), in 128 x NT output tiles
+// (NT = 256, or 64 for the first layer's weight gradient), optionally split
+// over K (weight gradients over the batch: each split writes its own FP32
+// partial tile).  Persistent: min(tiles, SMs) CTAs walk the tiles in a
+// static round robin.  Six warps, each with one job:
+//   warp 0     TMA producer: one lane issues cp.async.bulk.tensor loads of
+//              the 128 x 64 block of A and the NT x 64 block of B into a
+//              ring of shared-memory stages (128-byte swizzle, the canonical
+//              K-major layout the MMA reads), completing on the stage's
+//              "full" mbarrier;
+//   warp 1     MMA issuer: owns the tensor memory; one lane waits for a full
+//              stage, issues four tcgen05.mma (M=128, N=NT, K=16) into the
+//              tile's accumulator and commits them to the stage's "empty"
+//              mbarrier (the producer refills it when they complete); after
+//              the tile's last block it commits to the accumulator's "full"
+//              mbarrier;
+//   warps 2-5  epilogue: each warp owns the 32 tensor-memory lanes (tile
+//              rows) of its warp index mod 4; it reads 32 FP32 columns at a
+//              time with tcgen05.ld, applies the layer's epilogue, writes the
+//              32 x 32 block into a swizzled shared-memory staging buffer and
+//              stores it with a TMA tensor store (two buffers per warp).
+// The accumulator is double-buffered in tensor memory (2 x NT columns), so
+// the epilogue of one tile runs while the MMAs of the next tile do.
+// Epilogues:
+//   EPI_FWD  bias + ReLU -> bf16 row-major and (optionally) a transposed copy
 //   EPI_BWD  ReLU mask of the previous activation -> bf16 row-major / transposed
-//   EPI_F32  FP32 tile (split-K partials of weight gradients)
-// Every mbarrier wait is bounded (2 s of %globaltimer); on expiry the kernel
-// sets an error flag, waits once more (bounded) for its own MMAs, frees its
-// tensor memory and returns.
+//   EPI_F32  FP32 tile (the test GEMM; split-K partials of weight gradients)
+// No TMA load uses cluster multicast: every operand is this GPU's own memory
+// and each CTA loads its own tiles.
+// Every mbarrier wait is bounded (%globaltimer, 2 s by default).  A role
+// whose wait runs out sets the error flag and leaves its loop; the roles
+// waiting on it then run out too.  Before the tensor memory is freed the MMA
+// lane waits (bounded) for its own MMAs and the producer for its own loads,
+// so nothing is in flight when the CTA exits.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -41,10 +60,14 @@ typedef __nv_bfloat16 bf16;
 
 constexpr int BM = 128;
 constexpr int BK = 64;
-constexpr int THREADS = 128;
+#ifndef BGT_GEMM_EPI_WARPS
+#define BGT_GEMM_EPI_WARPS 8
+#endif
+constexpr int EPI_WARPS = BGT_GEMM_EPI_WARPS;  // 4 or 8: one or two warps per tensor-memory lane quarter
+constexpr int THREADS = 64 + 32 * EPI_WARPS;   // producer warp, MMA warp, epilogue warps
 constexpr int H = BGT_MLP_HIDDEN;
 constexpr int IN = BGT_MLP_IN;
-constexpr int KSPLIT = 128;  // samples per split-K chunk of a weight gradient
+constexpr int KSPLIT = 128;  // fewest samples per split-K chunk of a weight gradient
 
 // flat parameter layout
 constexpr int64_t OFF_W1 = 0;
@@ -65,14 +88,6 @@ enum { EPI_FWD = 0, EPI_BWD = 1, EPI_F32 = 2 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
@@ -80,6 +95,12 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 }
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t ok;
@@ -105,6 +126,33 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
     if (global_ns() - t0 > limit_ns) return false;
   }
   return true;
+}
+
+// TMA: 2-D tile load into shared memory, completing on an mbarrier (no
+// multicast), and 2-D tile store from shared memory in a bulk group
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int32_t x, int32_t y, uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// at most N of this thread's store groups still reading shared memory
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;\n" ::"n"(N) : "memory");
+}
+// all of this thread's store groups complete
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void prefetch_map(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
@@ -150,9 +198,32 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+// 64 consecutive FP32 columns of this thread's tensor-memory lane
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+      "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+      "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+        "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+        "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+        "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+        "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
 // Shared-memory matrix descriptor, K-major, 128-byte swizzle: start address
 // (>> 4), leading byte offset 1 (unused for swizzled K-major), stride byte
 // offset 1024 B between 8-row atoms, descriptor version 1, layout type 2.
+// The TMA's 128-byte swizzle writes exactly this layout: row r of a block
+// at r * 128 bytes, its 16-byte chunk c at chunk c ^ (r % 8).
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
@@ -167,180 +238,342 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
 // GEMM
 
 struct Epi {
-  const float* bias;        // EPI_FWD: [N]
-  bf16* out;                // EPI_FWD / EPI_BWD: row-major [M][ldo]
-  int64_t ldo;
-  bf16* out_t;              // optional transposed copy [N][ldt]
+  const float* bias;   // EPI_FWD: [N]
+  bf16* out_t;         // optional transposed copy [N][ldt] (EPI_FWD / EPI_BWD)
   int64_t ldt;
-  const bf16* mask;         // EPI_BWD: previous activation, row-major [M][ldm]
+  const bf16* mask;    // EPI_BWD: previous activation, row-major [M][ldm]
   int64_t ldm;
-  float* out_f32;           // EPI_F32: [gridDim.y][M][N]
 };
 
-// rows x 64 bf16 block of a row-major matrix into swizzled shared memory
-template <int ROWS>
-__device__ __forceinline__ void load_block(uint32_t s_base, const bf16* g, int64_t ld, int64_t row0, int64_t k0,
-                                           int tid) {
-#pragma unroll 4
-  for (int idx = tid; idx < ROWS * 8; idx += THREADS) {
-    const int r = idx >> 3, c = idx & 7;
-    const uint32_t dst = s_base + (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
-    cp_async16(dst, g + (row0 + r) * ld + k0 + c * 8);
-  }
-}
+template <int NT>
+struct GemmCfg {
+  static constexpr uint32_t A_BYTES = BM * BK * 2;
+  static constexpr uint32_t B_BYTES = NT * BK * 2;
+  static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr uint32_t EPI_BUF = 4096;  // 32 x 32 FP32 (or bf16) output block
+  static constexpr uint32_t TMEM_COLS = 2 * NT;
+  static constexpr int COLS_PER_WARP = NT / (EPI_WARPS / 4);  // accumulator columns one epilogue warp drains
+  // as many stages as fit next to two staging buffers per epilogue warp and
+  // the 1024-byte alignment slack (at most 6)
+  static constexpr int STAGES_FIT = (int)((232448u - EPI_WARPS * 2u * EPI_BUF - 1024u) / STAGE_BYTES);
+  static constexpr int STAGES = STAGES_FIT < 6 ? STAGES_FIT : 6;
+  static constexpr int SMEM = STAGES * STAGE_BYTES + EPI_WARPS * 2 * EPI_BUF + 1024;
+};
+static_assert(EPI_WARPS == 4 || EPI_WARPS == 8, "epilogue warps");
+static_assert(GemmCfg<256>::STAGES >= 3 && GemmCfg<64>::COLS_PER_WARP >= 32, "GEMM configuration");
+static_assert(GemmCfg<256>::SMEM <= 232448 && GemmCfg<64>::SMEM <= 232448, "shared memory per CTA");
 
 __device__ int g_gemm_error;
 
+// Tile t of a (m_tiles x splits) grid: rows mt * 128, K blocks [kb0, kb1)
+// of split sp.  Every split has at least one K block (host check).
+struct TileIdx {
+  int mt, sp, kb0, kb1;
+};
+__device__ __forceinline__ TileIdx tile_of(int t, int m_tiles, int splits, int kb_total) {
+  TileIdx r;
+  r.mt = t % m_tiles;
+  r.sp = t / m_tiles;
+  r.kb0 = (int)((int64_t)r.sp * kb_total / splits);
+  r.kb1 = (int)((int64_t)(r.sp + 1) * kb_total / splits);
+  return r;
+}
+
 template <int NT, int EPI>
 __global__ void __launch_bounds__(THREADS, 1)
-    gemm_kernel(const bf16* __restrict__ A, int64_t lda, const bf16* __restrict__ B, int64_t ldb, int k_blocks,
-                Epi ep, int* err, uint64_t wait_ns, int skip_mma) {
-  extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bars[2];
-  __shared__ uint32_t tmem_slot;
-  constexpr uint32_t A_BYTES = BM * BK * 2;
-  constexpr uint32_t B_BYTES = NT * BK * 2;
+    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ CUtensorMap tmC, int m_tiles, int splits, int kb_total, Epi ep, int* err,
+                uint64_t wait_ns, int skip_mma) {
+  using C = GemmCfg<NT>;
+  constexpr int S = C::STAGES;
   constexpr uint32_t IDESC = idesc_bf16(BM, NT);
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[S], empty_bar[S], acc_full[2], acc_empty[2], done_bar;
+  __shared__ uint32_t tmem_slot;
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
-  const uint32_t sA0 = base, sB0 = base + A_BYTES, sA1 = base + A_BYTES + B_BYTES, sB1 = sA1 + A_BYTES;
+  uint8_t* base_ptr = smem_raw + (base - smem_u32(smem_raw));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t row0 = (int64_t)blockIdx.x * BM;
-  const int64_t kbase = (int64_t)blockIdx.y * k_blocks * BK;
-  const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+  const int n_tiles = m_tiles * splits;
 
-  if (warp == 0) {
-    tmem_alloc(smem_u32(&tmem_slot), NT);
+  if (warp == 1) {
+    tmem_alloc(smem_u32(&tmem_slot), C::TMEM_COLS);
     tmem_relinquish();
   }
   if (tid == 0) {
-    mbar_init(bar0, 1);
-    mbar_init(bar1, 1);
+    for (int s = 0; s < S; s++) {
+      mbar_init(smem_u32(&full_bar[s]), 1);
+      mbar_init(smem_u32(&empty_bar[s]), 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(smem_u32(&acc_full[b]), 1);
+      mbar_init(smem_u32(&acc_empty[b]), EPI_WARPS);  // one arrival per epilogue warp
+    }
+    mbar_init(smem_u32(&done_bar), 1);
     fence_mbar_init();
+    prefetch_map(&tmA);
+    prefetch_map(&tmB);
+    prefetch_map(&tmC);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
-
   bool ok = true;
-  load_block<BM>(sA0, A, lda, row0, kbase, tid);
-  load_block<NT>(sB0, B, ldb, 0, kbase, tid);
-  cp_async_commit();
-  for (int kb = 0; kb < k_blocks; kb++) {
-    const int s = kb & 1;
-    if (kb + 1 < k_blocks) {
-      const int s1 = (kb + 1) & 1;
-      if (kb >= 1) {
-        // the MMAs of block kb-1 read stage s1: wait before refilling it
-        // (the outcome is made CTA-uniform before anyone leaves the loop)
-        const bool w = mbar_wait(s1 ? bar1 : bar0, ((kb - 1) >> 1) & 1, wait_ns);
-        if (!__syncthreads_and(w)) {
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int it = 0;  // loads issued
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const TileIdx ti = tile_of(t, m_tiles, splits, kb_total);
+        for (int kb = ti.kb0; kb < ti.kb1; kb++) {
+          const int s = it % S;
+          const uint32_t ph = (uint32_t)(it / S) & 1u;
+          // the stage's previous MMAs are done (the first pass waits on the
+          // phase before the barrier's first, which counts as complete)
+          if (!mbar_wait(smem_u32(&empty_bar[s]), ph ^ 1u, wait_ns)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = base + (uint32_t)s * C::STAGE_BYTES, sb = sa + C::A_BYTES;
+          const uint32_t fb = smem_u32(&full_bar[s]);
+          mbar_arrive_expect_tx(fb, C::STAGE_BYTES);
+          tma_load_2d(sa, &tmA, kb * BK, ti.mt * BM, fb);
+          tma_load_2d(sb, &tmB, kb * BK, 0, fb);
+          it++;
+        }
+      }
+      // every load issued has landed before the CTA can exit (bounded)
+      for (int s = 0; s < S && s < it; s++) {
+        const int last = it - 1 - ((it - 1 - s) % S);  // the last load into stage s
+        mbar_wait(smem_u32(&full_bar[s]), (uint32_t)(last / S) & 1u, wait_ns);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int it = 0, tc = 0;
+      bool issued = false;
+      for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, tc++) {
+        const TileIdx ti = tile_of(t, m_tiles, splits, kb_total);
+        const int b = tc & 1;
+        const uint32_t tph = (uint32_t)(tc >> 1) & 1u;
+        // the epilogue has drained this accumulator buffer
+        if (!mbar_wait(smem_u32(&acc_empty[b]), tph ^ 1u, wait_ns)) {
           ok = false;
           break;
         }
-      }
-      load_block<BM>(s1 ? sA1 : sA0, A, lda, row0, kbase + (int64_t)(kb + 1) * BK, tid);
-      load_block<NT>(s1 ? sB1 : sB0, B, ldb, 0, kbase + (int64_t)(kb + 1) * BK, tid);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    fence_proxy_async();
-    __syncthreads();
-    // skip_mma (tests only): no MMA and no commit are issued, so the
-    // mbarrier waits run out with nothing outstanding
-    if (tid == 0 && !skip_mma) {
-      tc_fence_after();
-      const uint32_t a_s = s ? sA1 : sA0, b_s = s ? sB1 : sB0;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(b * NT);
+        for (int kb = ti.kb0; kb < ti.kb1; kb++, it++) {
+          const int s = it % S;
+          if (!mbar_wait(smem_u32(&full_bar[s]), (uint32_t)(it / S) & 1u, wait_ns)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          // skip_mma (tests only): no MMA and no commit are issued, so the
+          // other roles' waits run out with nothing outstanding
+          if (!skip_mma) {
+            const uint32_t sa = base + (uint32_t)s * C::STAGE_BYTES, sb = sa + C::A_BYTES;
 #pragma unroll
-      for (int k = 0; k < BK / 16; k++) {
-        // K step of 16 bf16 = 32 bytes inside the 128-byte swizzle atom
-        mma_bf16(tmem, sw128_desc(a_s + k * 32), sw128_desc(b_s + k * 32), IDESC, (kb > 0 || k > 0) ? 1u : 0u);
-      }
-      mma_commit(s ? bar1 : bar0);
-    }
-  }
-  cp_async_wait<0>();
-  const int last = k_blocks - 1;
-  const uint32_t last_bar = (last & 1) ? bar1 : bar0;
-  if (ok) ok = mbar_wait(last_bar, (last >> 1) & 1, wait_ns);
-  ok = __syncthreads_and(ok);  // tcgen05.ld below is warp-collective
-  if (!ok) {
-    atomicExch(err, 1);
-    // bounded second wait for the MMAs in flight before tensor memory is freed
-    mbar_wait(last_bar, (last >> 1) & 1, wait_ns);
-  }
-  tc_fence_after();
-  __syncwarp();
-  if (ok) {
-    const int64_t row = row0 + warp * 32 + lane;
-    const uint32_t t_row = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-    for (int c0 = 0; c0 < NT; c0 += 32) {
-      uint32_t r[32];
-      tmem_ld32(t_row + c0, r);
-      float v[32];
-#pragma unroll
-      for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
-      if (EPI == EPI_F32) {
-        float4* dst = reinterpret_cast<float4*>(ep.out_f32 + ((int64_t)blockIdx.y * gridDim.x * BM + row) * NT + c0);
-#pragma unroll
-        for (int q = 0; q < 8; q++) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-      } else {
-        if (EPI == EPI_FWD) {
-#pragma unroll
-          for (int j = 0; j < 32; j++) v[j] = fmaxf(v[j] + ep.bias[c0 + j], 0.0f);
-        } else {
-          const uint4* mp = reinterpret_cast<const uint4*>(ep.mask + row * ep.ldm + c0);
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            uint4 u = mp[q];
-            const bf16* h = reinterpret_cast<const bf16*>(&u);
-#pragma unroll
-            for (int j = 0; j < 8; j++)
-              if (!(__bfloat162float(h[j]) > 0.0f)) v[8 * q + j] = 0.0f;
+            for (int k = 0; k < BK / 16; k++) {
+              // K step of 16 bf16 = 32 bytes inside the 128-byte swizzle atom
+              mma_bf16(d, sw128_desc(sa + k * 32), sw128_desc(sb + k * 32), IDESC,
+                       (kb > ti.kb0 || k > 0) ? 1u : 0u);
+            }
+            mma_commit(smem_u32(&empty_bar[s]));
+            issued = true;
           }
         }
-        uint4 pk[4];
-        bf16* ph = reinterpret_cast<bf16*>(pk);
+        if (!ok) break;
+        if (!skip_mma) mma_commit(smem_u32(&acc_full[b]));
+      }
+      // every MMA issued has completed before tensor memory is freed (bounded)
+      if (issued) {
+        mma_commit(smem_u32(&done_bar));
+        mbar_wait(smem_u32(&done_bar), 0u, wait_ns);
+      }
+    }
+  } else {
+    // ---------------- epilogue ----------------
+    const int q = warp & 3;  // tensor-memory lanes 32q .. 32q + 31 = tile rows
+    const int col0 = ((warp - 2) >> 2) * C::COLS_PER_WARP;  // this warp's accumulator columns
+    constexpr int GROUP = C::COLS_PER_WARP >= 64 ? 64 : 32;  // columns per tensor-memory load
+    const uint32_t ebuf = base + (uint32_t)S * C::STAGE_BYTES + (uint32_t)(warp - 2) * 2u * C::EPI_BUF;
+    uint8_t* ebuf_ptr = base_ptr + (size_t)S * C::STAGE_BYTES + (size_t)(warp - 2) * 2 * C::EPI_BUF;
+    int tc = 0, nst = 0;
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, tc++) {
+      const TileIdx ti = tile_of(t, m_tiles, splits, kb_total);
+      const int b = tc & 1;
+      const bool w = mbar_wait(smem_u32(&acc_full[b]), (uint32_t)(tc >> 1) & 1u, wait_ns);
+      if (!__all_sync(0xffffffffu, w)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int64_t row = (int64_t)ti.mt * BM + q * 32 + lane;  // this lane's output row
+      // row of the 32 x 32 store box in the output map
+      const int32_t ybox = (EPI == EPI_F32 ? ti.sp * m_tiles * BM : 0) + ti.mt * BM + q * 32;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * NT);
+#pragma unroll 1
+      for (int g0 = col0; g0 < col0 + C::COLS_PER_WARP; g0 += GROUP) {
+        uint32_t r[64];
+        if (GROUP == 64) {
+          tmem_ld64(taddr + g0, r);
+        } else {
+          tmem_ld32(taddr + g0, *reinterpret_cast<uint32_t(*)[32]>(r));
+        }
+        if (g0 + GROUP == col0 + C::COLS_PER_WARP) {
+          // this warp's part of the accumulator buffer is read: the next
+          // tile's MMAs may overwrite it
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+        }
 #pragma unroll
-        for (int j = 0; j < 32; j++) ph[j] = __float2bfloat16_rn(v[j]);
-        uint4* dst = reinterpret_cast<uint4*>(ep.out + row * ep.ldo + c0);
+        for (int h = 0; h < GROUP / 32; h++) {
+          const int c0 = g0 + 32 * h;
+          float v[32];
 #pragma unroll
-        for (int q = 0; q < 4; q++) dst[q] = pk[q];
-        if (ep.out_t) {
+          for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[32 * h + j]);
+          // staging buffer nst & 1: its previous store has finished reading it
+          if (lane == 0) bulk_wait_read<1>();
+          __syncwarp();
+          const uint32_t buf = ebuf + (uint32_t)(nst & 1) * C::EPI_BUF;
+          uint8_t* buf_ptr = ebuf_ptr + (size_t)(nst & 1) * C::EPI_BUF;
+          if (EPI == EPI_F32) {
+            // 32 rows x 128 bytes, 128-byte swizzle: chunk c of row r at c ^ (r % 8)
 #pragma unroll
-          for (int j = 0; j < 32; j++) ep.out_t[(int64_t)(c0 + j) * ep.ldt + row] = ph[j];
+            for (int c = 0; c < 8; c++)
+              *reinterpret_cast<float4*>(buf_ptr + lane * 128 + ((c ^ (lane & 7)) << 4)) =
+                  make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+          } else {
+            if (EPI == EPI_FWD) {
+#pragma unroll
+              for (int j = 0; j < 32; j++) v[j] = fmaxf(v[j] + ep.bias[c0 + j], 0.0f);
+            } else {
+              const uint4* mp = reinterpret_cast<const uint4*>(ep.mask + row * ep.ldm + c0);
+#pragma unroll
+              for (int c = 0; c < 4; c++) {
+                uint4 u = mp[c];
+                const bf16* hh = reinterpret_cast<const bf16*>(&u);
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                  if (!(__bfloat162float(hh[j]) > 0.0f)) v[8 * c + j] = 0.0f;
+              }
+            }
+            uint4 pk[4];
+            bf16* ph = reinterpret_cast<bf16*>(pk);
+#pragma unroll
+            for (int j = 0; j < 32; j++) ph[j] = __float2bfloat16_rn(v[j]);
+            // 32 rows x 64 bytes, 64-byte swizzle: chunk c of row r at c ^ ((r / 2) % 4)
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+              *reinterpret_cast<uint4*>(buf_ptr + lane * 64 + ((c ^ ((lane >> 1) & 3)) << 4)) = pk[c];
+            if (ep.out_t) {
+#pragma unroll
+              for (int j = 0; j < 32; j++) ep.out_t[(int64_t)(c0 + j) * ep.ldt + row] = ph[j];
+            }
+          }
+          fence_proxy_async();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_2d(&tmC, c0, ybox, buf);
+            bulk_commit();
+          }
+          nst++;
         }
       }
     }
+    if (lane == 0) bulk_wait_all();
   }
+  if (!ok) atomicExch(err, 1);
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, NT);
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, C::TMEM_COLS);
+  }
 }
 
-template <int NT>
-constexpr int gemm_smem() {
-  return 2 * (BM * BK * 2 + NT * BK * 2) + 1024;
+// ---------------------------------------------------------------------------
+// Tensor maps (driver entry point, resolved once through the runtime)
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
 }
 
+// 2-D map of a row-major matrix: `rows` rows of `cols` elements, `ld`
+// elements apart; boxes of box_rows x box_cols
+static bool make_map(CUtensorMap* map, CUtensorMapDataType dt, size_t esize, const void* ptr, uint64_t cols,
+                     uint64_t rows, uint64_t ld, uint32_t box_cols, uint32_t box_rows, CUtensorMapSwizzle sw) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {ld * esize};
+  const cuuint32_t box[2] = {box_cols, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(map, dt, 2, const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static int sm_count() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
+// C = A . B^T over K = k: A [a_rows][lda] bf16 (a_rows a multiple of 128),
+// B [NT][ldb] bf16, k a multiple of 64 split into `splits` chunks of whole
+// 64-blocks.  Output: EPI_F32 -> out FP32 [splits][a_rows][NT];
+// EPI_FWD / EPI_BWD -> out bf16 [a_rows][ldo] (columns 0..NT-1).
 template <int NT, int EPI>
-static cudaError_t launch_gemm(const bf16* A, int64_t lda, const bf16* B, int64_t ldb, int m_tiles, int splits,
-                               int k_blocks, const Epi& ep, int* err, cudaStream_t st,
+static cudaError_t launch_gemm(const bf16* A, int64_t lda, int64_t a_rows, const bf16* B, int64_t ldb, int64_t k,
+                               int splits, void* out, int64_t ldo, const Epi& ep, int* err, cudaStream_t st,
                                uint64_t wait_ns = 2000000000ull, int skip_mma = 0) {
+  using C = GemmCfg<NT>;
+  const int m_tiles = (int)(a_rows / BM);
+  const int kb_total = (int)(k / BK);
+  if (m_tiles <= 0 || kb_total <= 0 || splits <= 0 || splits > kb_total || a_rows % BM || k % BK)
+    return cudaErrorInvalidValue;
+  CUtensorMap ma, mb, mc;
+  bool good = make_map(&ma, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, A, (uint64_t)k, (uint64_t)a_rows, (uint64_t)lda,
+                       BK, BM, CU_TENSOR_MAP_SWIZZLE_128B) &&
+              make_map(&mb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, B, (uint64_t)k, (uint64_t)NT, (uint64_t)ldb, BK, NT,
+                       CU_TENSOR_MAP_SWIZZLE_128B);
+  if (EPI == EPI_F32)
+    good = good && make_map(&mc, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, out, (uint64_t)NT,
+                            (uint64_t)splits * (uint64_t)a_rows, (uint64_t)ldo, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B);
+  else
+    good = good && make_map(&mc, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, out, (uint64_t)NT, (uint64_t)a_rows,
+                            (uint64_t)ldo, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B);
+  if (!good) return cudaErrorInvalidValue;
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    cudaError_t e =
-        cudaFuncSetAttribute(gemm_kernel<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_smem<NT>());
+    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
     if (e != cudaSuccess) return e;
     attr_set[dev & 63] = true;
   }
-  gemm_kernel<NT, EPI><<<dim3(m_tiles, splits), THREADS, gemm_smem<NT>(), st>>>(A, lda, B, ldb, k_blocks, ep, err, wait_ns,
-                                                                              skip_mma);
+  const int grid = std::min(m_tiles * splits, sm_count());
+  gemm_kernel<NT, EPI><<<grid, THREADS, C::SMEM, st>>>(ma, mb, mc, m_tiles, splits, kb_total, ep, err, wait_ns,
+                                                       skip_mma);
   return cudaGetLastError();
 }
 
@@ -638,23 +871,18 @@ int bgt_mlp_set_params(bgt_mlp* m, const float* params) {
 // gradients and runs the loss head with labels
 static int forward_rows(bgt_mlp* m, const bf16* X, int64_t n, bool training, const float* label, float inv_batch,
                         float* prob, cudaStream_t st) {
-  const int tiles = (int)(n / BM);
   const int64_t ldt = m->max_batch;
   Epi e{};
   e.bias = m->params + OFF_B1;
-  e.out = m->a1;
-  e.ldo = H;
   e.out_t = training ? m->a1t : nullptr;
   e.ldt = ldt;
-  MCU(m, (launch_gemm<256, EPI_FWD>(X, IN, m->w1, IN, tiles, 1, IN / BK, e, m->d_err, st)));
+  MCU(m, (launch_gemm<256, EPI_FWD>(X, IN, n, m->w1, IN, IN, 1, m->a1, H, e, m->d_err, st)));
   e.bias = m->params + OFF_B2;
-  e.out = m->a2;
   e.out_t = training ? m->a2t : nullptr;
-  MCU(m, (launch_gemm<256, EPI_FWD>(m->a1, H, m->w2, H, tiles, 1, H / BK, e, m->d_err, st)));
+  MCU(m, (launch_gemm<256, EPI_FWD>(m->a1, H, n, m->w2, H, H, 1, m->a2, H, e, m->d_err, st)));
   e.bias = m->params + OFF_B3;
-  e.out = m->a3;
   e.out_t = nullptr;
-  MCU(m, (launch_gemm<256, EPI_FWD>(m->a2, H, m->w3, H, tiles, 1, H / BK, e, m->d_err, st)));
+  MCU(m, (launch_gemm<256, EPI_FWD>(m->a2, H, n, m->w3, H, H, 1, m->a3, H, e, m->d_err, st)));
   const int64_t threads = n * 32;
   head_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
       m->a3, n, m->params + OFF_W4, m->params + OFF_B4, label, inv_batch, prob, m->dlogit, m->dz3, m->dz3t, ldt,
@@ -674,7 +902,6 @@ static int check_error_flag(bgt_mlp* m) {
 // gradients of the mean loss over one batch into m->grads
 static int backward_batch(bgt_mlp* m, const bf16* X, const float* label, int32_t batch, cudaStream_t st) {
   const int64_t B = batch, ldt = m->max_batch;
-  const int tiles = (int)(B / BM);
   MCU(m, cudaMemsetAsync(m->scalars, 0, sizeof(float), st));
   transpose_in_kernel<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(X, B, m->xt, ldt);
   m->launches++;
@@ -682,21 +909,20 @@ static int backward_batch(bgt_mlp* m, const bf16* X, const float* label, int32_t
   if (rc) return rc;
   // dZ2 = (dZ3 . W3) * relu'(A2), dZ1 = (dZ2 . W2) * relu'(A1)
   Epi e{};
-  e.ldo = H;
   e.ldt = ldt;
   e.ldm = H;
-  e.out = m->dz2;
   e.out_t = m->dz2t;
   e.mask = m->a2;
-  MCU(m, (launch_gemm<256, EPI_BWD>(m->dz3, H, m->w3t, H, tiles, 1, H / BK, e, m->d_err, st)));
-  e.out = m->dz1;
+  MCU(m, (launch_gemm<256, EPI_BWD>(m->dz3, H, B, m->w3t, H, H, 1, m->dz2, H, e, m->d_err, st)));
   e.out_t = m->dz1t;
   e.mask = m->a1;
-  MCU(m, (launch_gemm<256, EPI_BWD>(m->dz2, H, m->w2t, H, tiles, 1, H / BK, e, m->d_err, st)));
-  // weight gradients dW = dZ^T . A_prev, split over the batch
-  const int splits = (int)(B / KSPLIT);
+  MCU(m, (launch_gemm<256, EPI_BWD>(m->dz2, H, B, m->w2t, H, H, 1, m->dz1, H, e, m->d_err, st)));
+  // weight gradients dW = dZ^T . A_prev over the batch, split into one
+  // chunk per CTA of a full wave (at least KSPLIT samples per chunk: the
+  // partial buffer holds max_batch / KSPLIT chunks); the FP32 partials are
+  // summed in a fixed order, so the gradients are deterministic
+  const int splits = (int)std::max<int64_t>(1, std::min<int64_t>(B / KSPLIT, sm_count() / (H / BM)));
   Epi f{};
-  f.out_f32 = m->partial;
   struct G {
     const bf16* dzt;
     const bf16* at;
@@ -705,9 +931,9 @@ static int backward_batch(bgt_mlp* m, const bf16* X, const float* label, int32_t
   } gs[3] = {{m->dz3t, m->a2t, OFF_W3, 256}, {m->dz2t, m->a1t, OFF_W2, 256}, {m->dz1t, m->xt, OFF_W1, 64}};
   for (const G& g : gs) {
     if (g.nt == 256)
-      MCU(m, (launch_gemm<256, EPI_F32>(g.dzt, ldt, g.at, ldt, H / BM, splits, KSPLIT / BK, f, m->d_err, st)));
+      MCU(m, (launch_gemm<256, EPI_F32>(g.dzt, ldt, H, g.at, ldt, B, splits, m->partial, 256, f, m->d_err, st)));
     else
-      MCU(m, (launch_gemm<64, EPI_F32>(g.dzt, ldt, g.at, ldt, H / BM, splits, KSPLIT / BK, f, m->d_err, st)));
+      MCU(m, (launch_gemm<64, EPI_F32>(g.dzt, ldt, H, g.at, ldt, B, splits, m->partial, 64, f, m->d_err, st)));
     const int64_t count = (int64_t)H * g.nt;
     reduce_kernel<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(m->partial, splits, count, m->grads + g.off);
     m->launches += 2;
@@ -819,12 +1045,11 @@ static int gemm_bf16(const uint16_t* d_a, int64_t lda, const uint16_t* d_b, int6
   if (cudaGetSymbolAddress((void**)&d_err, g_gemm_error) != cudaSuccess) return BGT_ECUDA;
   if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess) return BGT_ECUDA;
   Epi e{};
-  e.out_f32 = d_c;
   const bf16* A = reinterpret_cast<const bf16*>(d_a);
   const bf16* B = reinterpret_cast<const bf16*>(d_b);
   cudaError_t ce = (n == 256)
-                       ? launch_gemm<256, EPI_F32>(A, lda, B, ldb, m / BM, 1, k / BK, e, d_err, st, wait_ns, skip_mma)
-                       : launch_gemm<64, EPI_F32>(A, lda, B, ldb, m / BM, 1, k / BK, e, d_err, st, wait_ns, skip_mma);
+                       ? launch_gemm<256, EPI_F32>(A, lda, m, B, ldb, k, 1, d_c, n, e, d_err, st, wait_ns, skip_mma)
+                       : launch_gemm<64, EPI_F32>(A, lda, m, B, ldb, k, 1, d_c, n, e, d_err, st, wait_ns, skip_mma);
   if (ce != cudaSuccess) return BGT_ECUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return BGT_ECUDA;
   int flag = 0;

@@ -28,7 +28,8 @@ def _bf16(a, dev):
 
 
 @pytest.mark.parametrize("m,n,k", [(128, 64, 64), (256, 256, 256), (512, 256, 1024), (384, 64, 192),
-                                   (1024, 256, 64), (16384, 256, 256)])
+                                   (1024, 256, 64), (16384, 256, 256), (16384, 256, 4096), (37888, 64, 320),
+                                   (32768, 256, 128)])
 def test_gemm_matches_torch(m, n, k):
     from bgt import mlp
 
