@@ -245,23 +245,31 @@ struct Epi {
   int64_t ldm;
 };
 
-template <int NT>
+// Shared memory of one CTA: [stationary B: K <= 256, one split only]
+// [ring of STAGES stages: A block, and the B block when B is not stationary]
+// [one 32 x 32 output staging buffer per epilogue warp] + alignment slack.
+template <int NT, bool BRES>
 struct GemmCfg {
   static constexpr uint32_t A_BYTES = BM * BK * 2;
   static constexpr uint32_t B_BYTES = NT * BK * 2;
-  static constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int BRES_BLOCKS = 4;  // K blocks of a stationary B (K <= 256)
+  static constexpr uint32_t BRES_BYTES = BRES ? BRES_BLOCKS * B_BYTES : 0;
+  static constexpr uint32_t STAGE_BYTES = BRES ? A_BYTES : A_BYTES + B_BYTES;
   static constexpr uint32_t EPI_BUF = 4096;  // 32 x 32 FP32 (or bf16) output block
+  static constexpr uint32_t EPI_BYTES = EPI_WARPS * EPI_BUF;
   static constexpr uint32_t TMEM_COLS = 2 * NT;
   static constexpr int COLS_PER_WARP = NT / (EPI_WARPS / 4);  // accumulator columns one epilogue warp drains
-  // as many stages as fit next to two staging buffers per epilogue warp and
-  // the 1024-byte alignment slack (at most 6)
-  static constexpr int STAGES_FIT = (int)((232448u - EPI_WARPS * 2u * EPI_BUF - 1024u) / STAGE_BYTES);
+  // as many stages as fit (at most 6), leaving 2 KB for the static shared
+  // memory and 1 KB of alignment slack
+  static constexpr int STAGES_FIT = (int)((232448u - 2048u - EPI_BYTES - BRES_BYTES) / STAGE_BYTES);
   static constexpr int STAGES = STAGES_FIT < 6 ? STAGES_FIT : 6;
-  static constexpr int SMEM = STAGES * STAGE_BYTES + EPI_WARPS * 2 * EPI_BUF + 1024;
+  static constexpr int SMEM = BRES_BYTES + STAGES * STAGE_BYTES + EPI_BYTES + 1024;
 };
 static_assert(EPI_WARPS == 4 || EPI_WARPS == 8, "epilogue warps");
-static_assert(GemmCfg<256>::STAGES >= 3 && GemmCfg<64>::COLS_PER_WARP >= 32, "GEMM configuration");
-static_assert(GemmCfg<256>::SMEM <= 232448 && GemmCfg<64>::SMEM <= 232448, "shared memory per CTA");
+static_assert(GemmCfg<256, false>::STAGES >= 4 && GemmCfg<256, true>::STAGES >= 4 &&
+                  GemmCfg<64, false>::COLS_PER_WARP >= 32,
+              "GEMM configuration");
+static_assert(GemmCfg<256, false>::SMEM <= 230400 && GemmCfg<256, true>::SMEM <= 230400, "shared memory per CTA");
 
 __device__ int g_gemm_error;
 
@@ -279,25 +287,33 @@ __device__ __forceinline__ TileIdx tile_of(int t, int m_tiles, int splits, int k
   return r;
 }
 
-template <int NT, int EPI>
+// BRES: B (the layer's weights in the forward and backward-data GEMMs) is
+// loaded into shared memory once per CTA and stays there for all its tiles;
+// only A streams through the ring.  Needs one split and K <= 256.
+template <int NT, int EPI, bool BRES>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const __grid_constant__ CUtensorMap tmC, int m_tiles, int splits, int kb_total, Epi ep, int* err,
                 uint64_t wait_ns, int skip_mma) {
-  using C = GemmCfg<NT>;
+  using C = GemmCfg<NT, BRES>;
   constexpr int S = C::STAGES;
   constexpr uint32_t IDESC = idesc_bf16(BM, NT);
   extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[S], empty_bar[S], acc_full[2], acc_empty[2], done_bar;
+  __shared__ __align__(8) uint64_t full_bar[S], empty_bar[S], acc_full[2], acc_empty[2], done_bar, bres_bar;
   __shared__ uint32_t tmem_slot;
+  __shared__ __align__(16) float bias_s[EPI == EPI_FWD ? NT : 1];
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   uint8_t* base_ptr = smem_raw + (base - smem_u32(smem_raw));
+  const uint32_t ring = base + C::BRES_BYTES;  // stage s at ring + s * STAGE_BYTES
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n_tiles = m_tiles * splits;
 
   if (warp == 1) {
     tmem_alloc(smem_u32(&tmem_slot), C::TMEM_COLS);
     tmem_relinquish();
+  }
+  if (EPI == EPI_FWD) {
+    for (int j = tid; j < NT; j += THREADS) bias_s[j] = ep.bias[j];
   }
   if (tid == 0) {
     for (int s = 0; s < S; s++) {
@@ -309,6 +325,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(smem_u32(&acc_empty[b]), EPI_WARPS);  // one arrival per epilogue warp
     }
     mbar_init(smem_u32(&done_bar), 1);
+    mbar_init(smem_u32(&bres_bar), 1);
     fence_mbar_init();
     prefetch_map(&tmA);
     prefetch_map(&tmB);
@@ -323,7 +340,13 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
-      int it = 0;  // loads issued
+      if (BRES) {
+        // the stationary B: all its K blocks on one barrier
+        mbar_arrive_expect_tx(smem_u32(&bres_bar), (uint32_t)kb_total * C::B_BYTES);
+        for (int kb = 0; kb < kb_total; kb++)
+          tma_load_2d(base + (uint32_t)kb * C::B_BYTES, &tmB, kb * BK, 0, smem_u32(&bres_bar));
+      }
+      int it = 0;  // ring loads issued
       for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         const TileIdx ti = tile_of(t, m_tiles, splits, kb_total);
         for (int kb = ti.kb0; kb < ti.kb1; kb++) {
@@ -335,11 +358,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             ok = false;
             break;
           }
-          const uint32_t sa = base + (uint32_t)s * C::STAGE_BYTES, sb = sa + C::A_BYTES;
+          const uint32_t sa = ring + (uint32_t)s * C::STAGE_BYTES;
           const uint32_t fb = smem_u32(&full_bar[s]);
           mbar_arrive_expect_tx(fb, C::STAGE_BYTES);
           tma_load_2d(sa, &tmA, kb * BK, ti.mt * BM, fb);
-          tma_load_2d(sb, &tmB, kb * BK, 0, fb);
+          if (!BRES) tma_load_2d(sa + C::A_BYTES, &tmB, kb * BK, 0, fb);
           it++;
         }
       }
@@ -348,12 +371,14 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int last = it - 1 - ((it - 1 - s) % S);  // the last load into stage s
         mbar_wait(smem_u32(&full_bar[s]), (uint32_t)(last / S) & 1u, wait_ns);
       }
+      if (BRES) mbar_wait(smem_u32(&bres_bar), 0u, wait_ns);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       int it = 0, tc = 0;
       bool issued = false;
+      if (BRES && !mbar_wait(smem_u32(&bres_bar), 0u, wait_ns)) ok = false;
       for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x, tc++) {
         const TileIdx ti = tile_of(t, m_tiles, splits, kb_total);
         const int b = tc & 1;
@@ -375,7 +400,8 @@ __global__ void __launch_bounds__(THREADS, 1)
           // skip_mma (tests only): no MMA and no commit are issued, so the
           // other roles' waits run out with nothing outstanding
           if (!skip_mma) {
-            const uint32_t sa = base + (uint32_t)s * C::STAGE_BYTES, sb = sa + C::A_BYTES;
+            const uint32_t sa = ring + (uint32_t)s * C::STAGE_BYTES;
+            const uint32_t sb = BRES ? base + (uint32_t)kb * C::B_BYTES : sa + C::A_BYTES;
 #pragma unroll
             for (int k = 0; k < BK / 16; k++) {
               // K step of 16 bf16 = 32 bytes inside the 128-byte swizzle atom
@@ -400,24 +426,32 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int q = warp & 3;  // tensor-memory lanes 32q .. 32q + 31 = tile rows
     const int col0 = ((warp - 2) >> 2) * C::COLS_PER_WARP;  // this warp's accumulator columns
     constexpr int GROUP = C::COLS_PER_WARP >= 64 ? 64 : 32;  // columns per tensor-memory load
-    const uint32_t ebuf = base + (uint32_t)S * C::STAGE_BYTES + (uint32_t)(warp - 2) * 2u * C::EPI_BUF;
-    uint8_t* ebuf_ptr = base_ptr + (size_t)S * C::STAGE_BYTES + (size_t)(warp - 2) * 2 * C::EPI_BUF;
-    int tc = 0, nst = 0;
+    const uint32_t buf = ring + (uint32_t)S * C::STAGE_BYTES + (uint32_t)(warp - 2) * C::EPI_BUF;
+    uint8_t* buf_ptr = base_ptr + (buf - base);
+    int tc = 0;
     for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, tc++) {
       const TileIdx ti = tile_of(t, m_tiles, splits, kb_total);
       const int b = tc & 1;
+      const int64_t row = (int64_t)ti.mt * BM + q * 32 + lane;  // this lane's output row
       const bool w = mbar_wait(smem_u32(&acc_full[b]), (uint32_t)(tc >> 1) & 1u, wait_ns);
       if (!__all_sync(0xffffffffu, w)) {
         ok = false;
         break;
       }
       tc_fence_after();
-      const int64_t row = (int64_t)ti.mt * BM + q * 32 + lane;  // this lane's output row
       // row of the 32 x 32 store box in the output map
       const int32_t ybox = (EPI == EPI_F32 ? ti.sp * m_tiles * BM : 0) + ti.mt * BM + q * 32;
       const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * NT);
 #pragma unroll 1
       for (int g0 = col0; g0 < col0 + C::COLS_PER_WARP; g0 += GROUP) {
+        // EPI_BWD: the ReLU mask of this group's columns, requested before
+        // the tensor-memory load so the two latencies overlap
+        uint4 mk[GROUP / 8];
+        if (EPI == EPI_BWD) {
+          const uint4* mp = reinterpret_cast<const uint4*>(ep.mask + row * ep.ldm + g0);
+#pragma unroll
+          for (int c = 0; c < GROUP / 8; c++) mk[c] = mp[c];
+        }
         uint32_t r[64];
         if (GROUP == 64) {
           tmem_ld64(taddr + g0, r);
@@ -437,11 +471,9 @@ __global__ void __launch_bounds__(THREADS, 1)
           float v[32];
 #pragma unroll
           for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[32 * h + j]);
-          // staging buffer nst & 1: its previous store has finished reading it
-          if (lane == 0) bulk_wait_read<1>();
+          // the staging buffer's previous store has finished reading it
+          if (lane == 0) bulk_wait_read<0>();
           __syncwarp();
-          const uint32_t buf = ebuf + (uint32_t)(nst & 1) * C::EPI_BUF;
-          uint8_t* buf_ptr = ebuf_ptr + (size_t)(nst & 1) * C::EPI_BUF;
           if (EPI == EPI_F32) {
             // 32 rows x 128 bytes, 128-byte swizzle: chunk c of row r at c ^ (r % 8)
 #pragma unroll
@@ -451,13 +483,17 @@ __global__ void __launch_bounds__(THREADS, 1)
           } else {
             if (EPI == EPI_FWD) {
 #pragma unroll
-              for (int j = 0; j < 32; j++) v[j] = fmaxf(v[j] + ep.bias[c0 + j], 0.0f);
+              for (int c = 0; c < 8; c++) {
+                const float4 bb = *reinterpret_cast<const float4*>(&bias_s[c0 + 4 * c]);
+                v[4 * c] = fmaxf(v[4 * c] + bb.x, 0.0f);
+                v[4 * c + 1] = fmaxf(v[4 * c + 1] + bb.y, 0.0f);
+                v[4 * c + 2] = fmaxf(v[4 * c + 2] + bb.z, 0.0f);
+                v[4 * c + 3] = fmaxf(v[4 * c + 3] + bb.w, 0.0f);
+              }
             } else {
-              const uint4* mp = reinterpret_cast<const uint4*>(ep.mask + row * ep.ldm + c0);
 #pragma unroll
               for (int c = 0; c < 4; c++) {
-                uint4 u = mp[c];
-                const bf16* hh = reinterpret_cast<const bf16*>(&u);
+                const bf16* hh = reinterpret_cast<const bf16*>(&mk[4 * h + c]);
 #pragma unroll
                 for (int j = 0; j < 8; j++)
                   if (!(__bfloat162float(hh[j]) > 0.0f)) v[8 * c + j] = 0.0f;
@@ -482,7 +518,6 @@ __global__ void __launch_bounds__(THREADS, 1)
             tma_store_2d(&tmC, c0, ybox, buf);
             bulk_commit();
           }
-          nst++;
         }
       }
     }
@@ -538,15 +573,35 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
+template <int NT, int EPI, bool BRES>
+static cudaError_t launch_gemm_kernel(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mc, int m_tiles,
+                                      int splits, int kb_total, const Epi& ep, int* err, cudaStream_t st,
+                                      uint64_t wait_ns, int skip_mma) {
+  using C = GemmCfg<NT, BRES>;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    cudaError_t e =
+        cudaFuncSetAttribute(gemm_kernel<NT, EPI, BRES>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set[dev & 63] = true;
+  }
+  const int grid = std::min(m_tiles * splits, sm_count());
+  gemm_kernel<NT, EPI, BRES><<<grid, THREADS, C::SMEM, st>>>(ma, mb, mc, m_tiles, splits, kb_total, ep, err, wait_ns,
+                                                             skip_mma);
+  return cudaGetLastError();
+}
+
 // C = A . B^T over K = k: A [a_rows][lda] bf16 (a_rows a multiple of 128),
 // B [NT][ldb] bf16, k a multiple of 64 split into `splits` chunks of whole
 // 64-blocks.  Output: EPI_F32 -> out FP32 [splits][a_rows][NT];
-// EPI_FWD / EPI_BWD -> out bf16 [a_rows][ldo] (columns 0..NT-1).
+// EPI_FWD / EPI_BWD -> out bf16 [a_rows][ldo] (columns 0..NT-1).  With one
+// split and K <= 256 the kernel keeps B stationary in shared memory.
 template <int NT, int EPI>
 static cudaError_t launch_gemm(const bf16* A, int64_t lda, int64_t a_rows, const bf16* B, int64_t ldb, int64_t k,
                                int splits, void* out, int64_t ldo, const Epi& ep, int* err, cudaStream_t st,
                                uint64_t wait_ns = 2000000000ull, int skip_mma = 0) {
-  using C = GemmCfg<NT>;
   const int m_tiles = (int)(a_rows / BM);
   const int kb_total = (int)(k / BK);
   if (m_tiles <= 0 || kb_total <= 0 || splits <= 0 || splits > kb_total || a_rows % BM || k % BK)
@@ -563,18 +618,9 @@ static cudaError_t launch_gemm(const bf16* A, int64_t lda, int64_t a_rows, const
     good = good && make_map(&mc, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, out, (uint64_t)NT, (uint64_t)a_rows,
                             (uint64_t)ldo, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B);
   if (!good) return cudaErrorInvalidValue;
-  static bool attr_set[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!attr_set[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_kernel<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
-    if (e != cudaSuccess) return e;
-    attr_set[dev & 63] = true;
-  }
-  const int grid = std::min(m_tiles * splits, sm_count());
-  gemm_kernel<NT, EPI><<<grid, THREADS, C::SMEM, st>>>(ma, mb, mc, m_tiles, splits, kb_total, ep, err, wait_ns,
-                                                       skip_mma);
-  return cudaGetLastError();
+  if (splits == 1 && kb_total <= GemmCfg<NT, true>::BRES_BLOCKS)
+    return launch_gemm_kernel<NT, EPI, true>(ma, mb, mc, m_tiles, splits, kb_total, ep, err, st, wait_ns, skip_mma);
+  return launch_gemm_kernel<NT, EPI, false>(ma, mb, mc, m_tiles, splits, kb_total, ep, err, st, wait_ns, skip_mma);
 }
 
 // ---------------------------------------------------------------------------
