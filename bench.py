@@ -54,9 +54,11 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="use the library's default launch shape")
     ap.add_argument("--tuning", default="", help="threads_per_block,blocks_per_sm (skips the autotuner); DA "
                     "workloads also take ,table_mode[,compact_every]")
-    ap.add_argument("--workload", default="track", choices=["track", "da", "learned-da", "sext-scan"],
+    ap.add_argument("--workload", default="track", choices=["track", "da", "learned-da", "sext-scan", "mlp"],
                     help="track: the headline tracking metric (default); da: batched DA scan of error variants; "
-                         "learned-da: classifier-pruned vs plain DA scan; sext-scan: pruned sextupole-setting scan")
+                         "learned-da: classifier-pruned vs plain DA scan; sext-scan: pruned sextupole-setting scan; "
+                         "mlp: the survival classifier's tensor-core forward pass and training step")
+    ap.add_argument("--mlp-rows", type=int, default=262144, help="mlp: rows of one forward pass")
     ap.add_argument("--variants", type=int, default=0, help="DA workloads: number of lattice variants")
     ap.add_argument("--da-turns", type=int, default=0, help="DA workloads: turns per probe (default 20000)")
     ap.add_argument("--jitter", action="store_true", help="learned-da: add one jittered probe per grid cell")
@@ -430,7 +432,8 @@ def run_learned_da(args):
     with ClockSampler(R.local) as clk:
         jit = (None, args.seed) if args.jitter else (None,)
         pb_tr, scans, train_scan_s = _staged_scan_sharded(R, lats, rings.CONFIG2_GRID, turns, half, jit, tun)
-        net = SurvivalMLP(max_batch=16384, seed=args.seed)
+        # 65,536-row inference chunks: several tiles per CTA in each GEMM launch
+        net = SurvivalMLP(max_batch=65536, seed=args.seed)
         train = _train_classifier(args, R, pb_tr, scans, net)
         R.barrier()
         plain = da.sharded_scan(lambda b, e: da.plain_scan(pb_te.tracker, pb_te.ref, **pb_te.grid()), nv - half,
@@ -522,7 +525,7 @@ def run_sext_scan(args):
     t_setup = time.perf_counter() - t0
     tun = _autotune_da(pb_rest, fixed=args.tuning)
     pb_aud.tracker.set_tuning(**tun)
-    net = SurvivalMLP(max_batch=16384, seed=args.seed)
+    net = SurvivalMLP(max_batch=65536, seed=args.seed)
     fine = bool(args.model)
     if fine:
         net.load(args.model)
@@ -567,10 +570,84 @@ def run_sext_scan(args):
     R.close()
 
 
+def run_mlp(args):
+    """The survival classifier on its own: one step = 200 forward passes over
+    --mlp-rows probes each (three tcgen05 GEMM layers and the output head, in
+    65,536-row chunks; 200 passes so the clock sampler sees the timed region)
+    and, separately, 200 Adam training steps on an 8,192-sample batch; CUDA
+    events on the launching stream.  Beside it the same three layers as torch
+    bf16 matmuls (cuBLAS) with ReLU, for context."""
+    import torch
+
+    from bgt.mlp import SurvivalMLP
+
+    dev = torch.device("cuda", 0)
+    rows = args.mlp_rows
+    net = SurvivalMLP(max_batch=65536, seed=args.seed)
+    g = torch.Generator(device="cpu").manual_seed(args.seed)
+    x = (torch.randn(rows, 64, generator=g) * 0.5).to(dev).to(torch.bfloat16)
+    xb = x[:8192].contiguous()
+    yb = (torch.rand(8192, generator=g) < 0.3).float().to(dev)
+
+    passes = 200
+
+    def timed(fn, steps, warmup):
+        """ms per pass"""
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps * passes):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / (steps * passes)
+
+    fwd_flops = 2.0 * rows * (64 * 256 + 2 * 256 * 256)
+    train_flops = 852_000.0 * 8192  # forward + backward GEMM flops per sample x batch
+    l0 = net.launch_count
+    with ClockSampler(0) as clk:
+        ms_fwd = timed(lambda: net.forward(x), args.steps, args.warmup)
+        l1 = net.launch_count
+        ms_train = timed(lambda: net.train_step(xb, yb, 1e-4), args.steps, args.warmup)
+    per_pass = (l1 - l0) // max(1, args.steps * passes + args.warmup)  # the library's kernels in one forward pass
+    w = [(torch.randn(256, k, generator=g) * 0.05).to(dev).to(torch.bfloat16) for k in (64, 256, 256)]
+
+    def torch_fwd():
+        a = x
+        for wi in w:
+            a = torch.relu(a @ wi.T)
+        return a
+
+    ms_torch = timed(torch_fwd, args.steps, args.warmup)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    tf = fwd_flops / (ms_fwd * 1e-3) / 1e12
+    line = {"metric": "survival-classifier forward pass, tcgen05 BF16 GEMMs (FP32 accumulation)",
+            "value": tf, "unit": "TFLOP/s", "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_fwd * passes, "ms_per_forward": ms_fwd, "dtype": "bf16",
+            "data": "synthetic",
+            "config": {"workload": "64-256-256-256-1 MLP forward", "rows": rows, "chunk_rows": 65536,
+                       "passes_per_step": passes},
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"},
+            "train_step": {"batch": 8192, "ms": ms_train,
+                           "tflops": train_flops / (ms_train * 1e-3) / 1e12},
+            "torch_cublas_forward_ms": ms_torch, "gpu_launches": per_pass * passes * args.steps,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload != "track":
-        {"da": run_da, "learned-da": run_learned_da, "sext-scan": run_sext_scan}[args.workload](args)
+        {"da": run_da, "learned-da": run_learned_da, "sext-scan": run_sext_scan,
+         "mlp": run_mlp}[args.workload](args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -102,7 +102,7 @@ def pad_rows(n: int) -> int:
 
 
 class SurvivalMLP:
-    def __init__(self, max_batch: int = 16384, seed: int = 1, device: int = 0):
+    def __init__(self, max_batch: int = 65536, seed: int = 1, device: int = 0):
         self.lib = _bind()
         self.device = device
         self.max_batch = max_batch
