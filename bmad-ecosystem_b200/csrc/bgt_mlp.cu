@@ -4,12 +4,15 @@
 // accumulators in tensor memory), the output layer / loss / Adam on CUDA
 // cores.  C ABI in include/bgt_mlp.h.  No counterpart in the reference.
 //
-// GEMM kernel (gemm_kernel<NT, EPI>): C = A[M][K] . B[NT][K]^T with both
-// operands K-major (row-major, K contiguous), in 128 x NT output tiles
+// GEMM kernel (gemm_kernel<NT, EPI, BRES>): C = A[M][K] . B[NT][K]^T with
+// both operands K-major (row-major, K contiguous), in 128 x NT output tiles
 // (NT = 256, or 64 for the first layer's weight gradient), optionally split
 // over K (weight gradients over the batch: each split writes its own FP32
 // partial tile).  Persistent: min(tiles, SMs) CTAs walk the tiles in a
-// static round robin.  Six warps, each with one job:
+// static round robin.  BRES (one split, K <= 256: the forward and
+// backward-data layers, where B is the layer's weights): B is loaded into
+// shared memory once per CTA and only A streams through the ring.  Ten
+// warps, each with one job:
 //   warp 0     TMA producer: one lane issues cp.async.bulk.tensor loads of
 //              the 128 x 64 block of A and the NT x 64 block of B into a
 //              ring of shared-memory stages (128-byte swizzle, the canonical
@@ -21,11 +24,13 @@
 //              mbarrier (the producer refills it when they complete); after
 //              the tile's last block it commits to the accumulator's "full"
 //              mbarrier;
-//   warps 2-5  epilogue: each warp owns the 32 tensor-memory lanes (tile
-//              rows) of its warp index mod 4; it reads 32 FP32 columns at a
-//              time with tcgen05.ld, applies the layer's epilogue, writes the
-//              32 x 32 block into a swizzled shared-memory staging buffer and
-//              stores it with a TMA tensor store (two buffers per warp).
+//   warps 2-9  epilogue: each warp owns the 32 tensor-memory lanes (tile
+//              rows) of its warp index mod 4 and half of the columns; it
+//              reads 64 FP32 columns at a time with tcgen05.ld, applies the
+//              layer's epilogue (bias from shared memory; the ReLU mask
+//              requested before the tensor-memory load), writes each 32 x 32
+//              block into its swizzled shared-memory staging buffer and
+//              stores it with a TMA tensor store.
 // The accumulator is double-buffered in tensor memory (2 x NT columns), so
 // the epilogue of one tile runs while the MMAs of the next tile do.
 // Epilogues:
