@@ -12,6 +12,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -595,6 +596,44 @@ static int ensure_pinned(bgt_handle* h, CallCtx* c, size_t bytes) {
 // Host-buffer tracking shared by bgt_track_turns and bgt_track_elements: the
 // particles go through the context's pinned staging buffer to its device
 // buffers on its own stream; the call waits for that stream only.
+// Copies between the caller's (pageable) host buffers and the pinned
+// staging buffer.  One core copies pageable memory at a few GB/s, well below
+// the host link, so large calls split the bytes evenly over up to 8 threads.
+struct HostCopy {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+static void host_copies(const std::vector<HostCopy>& jobs) {
+  size_t total = 0;
+  for (const HostCopy& j : jobs) total += j.bytes;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = (int)std::min<size_t>(std::min(8u, hw), total / ((size_t)4 << 20));
+  auto piece = [&](int k, int parts) {
+    const size_t lo = total * k / parts, hi = total * (k + 1) / parts;
+    size_t off = 0;
+    for (const HostCopy& j : jobs) {
+      const size_t a = std::max(lo, off), b = std::min(hi, off + j.bytes);
+      if (a < b) memcpy((char*)j.dst + (a - off), (const char*)j.src + (a - off), b - a);
+      off += j.bytes;
+    }
+  };
+  if (nt <= 1) {
+    piece(0, 1);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int k = 1; k < nt; k++) {
+    try {
+      th.emplace_back(piece, k, nt);
+    } catch (...) {
+      piece(k, nt);  // no thread available: this one copies the piece
+    }
+  }
+  piece(0, nt);
+  for (std::thread& t : th) t.join();
+}
+
 static int track_host(bgt_handle* h, double* vec6, double* beta, void* t, int32_t* state, int32_t* ixe, int32_t* ixt,
                       const int32_t* variant, int64_t n, int32_t turn0, int32_t n_turns, int32_t rec_begin,
                       int32_t rec_end) {
@@ -656,16 +695,14 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, void* t, int32_
   int32_t* p_slot = p_t + n;
   int32_t* p_tv = p_slot + (multi ? n_slots : 0);
   int32_t* p_flag = p_tv + (multi ? tile_var.size() : 0);
-  if (t) memcpy(p_time, t, b_t);
-  memcpy(p_v, vec6, b_v);
-  memcpy(p_b, beta, b_b);
-  memcpy(p_s, state, b_i);
-  memcpy(p_e, ixe, b_i);
-  if (ixt) memcpy(p_t, ixt, b_i);
-  if (multi) {
-    memcpy(p_slot, slot_map.data(), b_slot);
-    memcpy(p_tv, tile_var.data(), b_tv);
-  }
+  host_copies({{p_time, t, b_t},
+               {p_v, vec6, b_v},
+               {p_b, beta, b_b},
+               {p_s, state, b_i},
+               {p_e, ixe, b_i},
+               {p_t, ixt, ixt ? b_i : 0},
+               {p_slot, slot_map.data(), b_slot},
+               {p_tv, tile_var.data(), b_tv}});
   int32_t* d_state = c->d_i32;
   int32_t* d_ixe = d_state + c->cap;
   int32_t* d_ixt = d_ixe + c->cap;
@@ -698,12 +735,12 @@ static int track_host(bgt_handle* h, double* vec6, double* beta, void* t, int32_
   if (ixt) CU(h, cudaMemcpyAsync(p_t, d_ixt, b_i, cudaMemcpyDeviceToHost, st));
   CU(h, cudaStreamSynchronize(st));
   if (*p_flag) return set_err(h, BGT_ETIMEOUT, "element-table staging did not complete");
-  if (t) memcpy(t, p_time, b_t);
-  memcpy(vec6, p_v, b_v);
-  memcpy(beta, p_b, b_b);
-  memcpy(state, p_s, b_i);
-  memcpy(ixe, p_e, b_i);
-  if (ixt) memcpy(ixt, p_t, b_i);
+  host_copies({{t, p_time, b_t},
+               {vec6, p_v, b_v},
+               {beta, p_b, b_b},
+               {state, p_s, b_i},
+               {ixe, p_e, b_i},
+               {ixt, p_t, ixt ? b_i : 0}});
   return 0;
 }
 
