@@ -225,6 +225,53 @@ def staged_scan(pb: ScanProblem, v_begin: int, v_end: int, early: int = 64, n_tu
     return StagedScan(vec0, snap, var, alive, surv, early, nt, wall, pt)
 
 
+def compacted_scan(pb: ScanProblem, v_begin: int, v_end: int, early: int = 64, n_turns: Optional[int] = None,
+                   retune_subset: bool = True) -> da.DAResult:
+    """Plain scan of variants [v_begin, v_end) in two launches and no
+    classifier: every probe `early` turns, then only the probes still alive,
+    packed densely in tracking order (variants stay sorted), to the full
+    turn count.  On the error rings ~70 % of the probes are lost within the
+    first turns; in a one-launch scan their lanes stay in the tiles of the
+    long-lived probes, here the second launch holds live probes only.  Each
+    probe's arithmetic does not depend on its lane, so the outcomes equal
+    the one-launch scan's bit for bit.  With `retune_subset` the second
+    launch's shape is re-tuned on the packed set (a few 2-turn trial
+    launches) and the tracker's tuning restored afterwards."""
+    import torch
+
+    nt = pb.n_turns if n_turns is None else n_turns
+    nv = v_end - v_begin
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    vec0, var = grid_probes(pb, v_begin, v_end)
+    tr = pb.tracker
+    b = _Bunch(vec0, var, tr.p0c, tr.species.mass, tracking_order(pb, nv))
+    b.track(tr, early, 0)
+    idx = torch.nonzero(b.state == 1).view(-1)  # tracking positions, ascending
+    if idx.numel() and nt > early:
+        sub = b.subset(idx)
+        saved = tr.get_tuning()
+        if retune_subset:
+            from . import autotune
+
+            autotune.tune(tr, sub.vec.cpu().numpy(), turns=2, sample=int(idx.numel()), variant=sub.var.cpu().numpy())
+        sub.track(tr, nt - early, early)
+        tr.set_tuning(**saved)
+        b.state[idx] = sub.state
+        b.ixt[idx] = sub.ixt
+        b.ixe[idx] = sub.ixe
+        b.vec[:, idx] = sub.vec
+    surv = b.probe_order(survive_turns(b.state, b.ixt, nt))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    s = surv.cpu().numpy().astype(np.int32)
+    radius = radius_of(pb, s >= nt, nv)
+    pt = int(np.minimum(s, nt).sum())
+    return da.DAResult(radius, s.reshape(nv, len(pb.deltas), pb.n_angle, pb.n_radius),
+                       da.ray_angles(pb.n_angle, pb.angle_min, pb.angle_max), da.grid_radii(pb.n_radius, pb.r_max),
+                       nt, wall, pt)
+
+
 def radius_of(pb: ScanProblem, survive_label, nv: int) -> np.ndarray:
     """DA radius per ray from a boolean survive label per probe."""
     s = np.asarray(survive_label).reshape(nv, len(pb.deltas), pb.n_angle, pb.n_radius)

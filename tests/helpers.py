@@ -272,7 +272,7 @@ def result_digest(vec6, beta, state, ix_ele_lost, ix_turn_lost) -> str:
 def plain_rel_err(g: np.ndarray, o: np.ndarray) -> np.ndarray:
     """Per particle, the largest plain per-coordinate relative error
     max_c |g_c - o_c| / |o_c| (0 where the values are equal, inf where o_c is
-    0 and g_c is not): the north_star's "relative per coordinate" with no
+    0 and g_c is not): "relative per coordinate" as the parity bounds state it, with no
     floor, so a coordinate passing near zero counts at its own size."""
     d = np.abs(np.asarray(g, np.float64) - np.asarray(o, np.float64))
     with np.errstate(divide="ignore", invalid="ignore"):

@@ -8,7 +8,7 @@ apertures and beam (20,000 of its particles, 1000 turns).
   the glibc one, minutes at these sizes).
 * Against the glibc oracle build (the reference's arithmetic), run here:
   states, loss elements and loss turns exact; coordinates within
-  north_star's bounds -- 1e-13 after one turn, 1e-9 after 1000 turns,
+  the tracker's parity bounds -- 1e-13 after one turn, 1e-9 after 1000 turns,
   relative per coordinate -- for every particle except those on which the
   two CPU builds of the oracle already differ by more than the bound (glibc
   not correctly rounded on a fraction of asin/sin/atan2 arguments, amplified

@@ -162,3 +162,26 @@ def test_staged_scan_equals_one_launch_scan(variants):
     plain = da.plain_scan(pb.tracker, pb.ref, **pb.grid())
     assert np.array_equal(st.survive.cpu().numpy(), plain.survive_turns.reshape(-1))
     assert np.any(plain.survive_turns < 90) and np.any(plain.survive_turns == 90)
+
+
+@pytest.mark.parametrize("retune", [False, True])
+def test_compacted_scan_equals_one_launch_scan(variants, retune):
+    """The compacted plain scan (every probe 5 turns, then the live probes
+    packed densely, optionally with a re-tuned launch shape) gives the
+    one-launch scan's survival turns, radii and particle.turns exactly, with
+    losses in both launches."""
+    from bgt import da, rings
+    from bgt import learned_da as LD
+    from bgt.track import Tracker
+
+    grid = rings.DAGrid(6, 16, 0.03, (-0.01, 0.0), 90)
+    pb = LD.setup(Tracker(variants), variants, grid)
+    tun = pb.tracker.get_tuning()
+    cs = LD.compacted_scan(pb, 0, 3, early=5, retune_subset=retune)
+    assert pb.tracker.get_tuning() == tun  # the scan's tuning is restored
+    plain = da.plain_scan(pb.tracker, pb.ref, **pb.grid())
+    assert np.array_equal(cs.survive_turns, plain.survive_turns)
+    assert np.array_equal(cs.radius, plain.radius)
+    assert cs.particle_turns == plain.particle_turns
+    s = plain.survive_turns
+    assert np.any(s < 5) and np.any((s >= 5) & (s < 90)) and np.any(s == 90)

@@ -162,3 +162,34 @@ def test_training_learns_a_separable_rule():
     p = net.forward(xt).cpu().numpy()
     acc = float(np.mean((p > 0.5) == (y > 0.5)))
     assert hist[-1] < 0.5 * l0 and acc > 0.95, (l0, hist, acc)
+
+
+def test_forward_and_gradients_with_several_tiles_per_cta():
+    """The classifier runs its GEMMs on 65,536-row chunks, where each
+    persistent CTA drains several 128-row tiles through the double-buffered
+    tensor-memory accumulators with the weights held in shared memory: the
+    forward pass (bias + ReLU epilogue) on 65,536 rows and the gradients on a
+    32,768-sample batch (ReLU-mask epilogue, 74 weight-gradient splits)
+    against the oracle, with the single-tile tests' tolerances."""
+    from bgt import mlp
+
+    dev = torch.device("cuda", 0)
+    p, X, y = _random_net(seed=12, n=65536)
+    net = mlp.SurvivalMLP(max_batch=65536, seed=1)
+    net.set_params(p)
+    prob = net.forward(_bf16(X, dev)).cpu().numpy()
+    ref = M.forward(p, X, emulate=True)["p"]
+    assert np.max(np.abs(prob - ref)) < 2e-3
+    assert np.mean(np.abs(prob - ref)) < 2e-4
+    Xb, yb = X[:32768], y[:32768]
+    g, loss = net.gradients(_bf16(Xb, dev), torch.tensor(yb, device=dev))
+    g = g.cpu().numpy().astype(np.float64)
+    gr, lr_ = M.gradients(p, Xb, yb.astype(np.float64), emulate=True)
+    assert abs(loss - lr_) < 1e-4
+    for a, b in ((M.OFF_W1, M.OFF_B1), (M.OFF_B1, M.OFF_W2), (M.OFF_W2, M.OFF_B2), (M.OFF_B2, M.OFF_W3),
+                 (M.OFF_W3, M.OFF_B3), (M.OFF_B3, M.OFF_W4), (M.OFF_W4, M.OFF_B4), (M.OFF_B4, M.N_PARAMS)):
+        d, r = g[a:b], gr[a:b]
+        rel = np.linalg.norm(d - r) / max(np.linalg.norm(r), 1e-30)
+        cos = float(d @ r / (np.linalg.norm(d) * np.linalg.norm(r) + 1e-300))
+        assert rel < 1e-2, (a, rel)
+        assert cos > 0.9999 or b - a == 1, (a, cos)
