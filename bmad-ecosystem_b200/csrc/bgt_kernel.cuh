@@ -5,7 +5,7 @@
 // Launch model: one thread per particle, the particle's phase-space vector in
 // registers for whole turns.  A CTA owns a tile of particles ("slots") of one
 // lattice variant; it stages that variant's element table into shared memory
-// with one bulk TMA copy (cp.async.bulk, no multicast) completed on an
+// with one bulk TMA copy (cp.async.bulk into its own shared memory) completed on an
 // mbarrier, then walks turns x records reading the table by broadcast.  The
 // grid is persistent (a multiple of the SM count); CTAs pull tiles from an
 // atomic counter so uneven survival balances across SMs.  Every few turns a

@@ -37,8 +37,8 @@
 //   EPI_FWD  bias + ReLU -> bf16 row-major and (optionally) a transposed copy
 //   EPI_BWD  ReLU mask of the previous activation -> bf16 row-major / transposed
 //   EPI_F32  FP32 tile (the test GEMM; split-K partials of weight gradients)
-// No TMA load uses cluster multicast: every operand is this GPU's own memory
-// and each CTA loads its own tiles.
+// Every TMA load is a plain per-CTA load of this GPU's own memory: each CTA
+// loads its own tiles, none is shared across a cluster.
 // Every mbarrier wait is bounded (%globaltimer, 2 s by default).  A role
 // whose wait runs out sets the error flag and leaves its loop; the roles
 // waiting on it then run out too.  Before the tensor memory is freed the MMA
@@ -133,8 +133,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_
   return true;
 }
 
-// TMA: 2-D tile load into shared memory, completing on an mbarrier (no
-// multicast), and 2-D tile store from shared memory in a bulk group
+// TMA: 2-D tile load into this CTA's shared memory, completing on an
+// mbarrier, and 2-D tile store from shared memory in a bulk group
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y, uint32_t bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
