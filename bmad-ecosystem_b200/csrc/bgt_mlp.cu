@@ -317,6 +317,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     tmem_alloc(smem_u32(&tmem_slot), C::TMEM_COLS);
     tmem_relinquish();
   }
+  // Launched as a programmatic dependent of the previous kernel on the
+  // stream: everything above runs while that kernel drains; no global
+  // memory is touched before the previous grid has completed and its writes
+  // are visible.  Then this grid lets the next one begin its own launch.
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   if (EPI == EPI_FWD) {
     for (int j = tid; j < NT; j += THREADS) bias_s[j] = ep.bias[j];
   }
@@ -593,9 +599,18 @@ static cudaError_t launch_gemm_kernel(const CUtensorMap& ma, const CUtensorMap& 
     attr_set[dev & 63] = true;
   }
   const int grid = std::min(m_tiles * splits, sm_count());
-  gemm_kernel<NT, EPI, BRES><<<grid, THREADS, C::SMEM, st>>>(ma, mb, mc, m_tiles, splits, kb_total, ep, err, wait_ns,
-                                                             skip_mma);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = C::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, gemm_kernel<NT, EPI, BRES>, ma, mb, mc, m_tiles, splits, kb_total, ep, err,
+                            wait_ns, skip_mma);
 }
 
 // C = A . B^T over K = k: A [a_rows][lda] bf16 (a_rows a multiple of 128),
