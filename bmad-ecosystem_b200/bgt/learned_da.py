@@ -251,12 +251,15 @@ def compacted_scan(pb: ScanProblem, v_begin: int, v_end: int, early: int = 64, n
     if idx.numel() and nt > early:
         sub = b.subset(idx)
         saved = tr.get_tuning()
-        if retune_subset:
-            from . import autotune
+        try:
+            if retune_subset:
+                from . import autotune
 
-            autotune.tune(tr, sub.vec.cpu().numpy(), turns=2, sample=int(idx.numel()), variant=sub.var.cpu().numpy())
-        sub.track(tr, nt - early, early)
-        tr.set_tuning(**saved)
+                autotune.tune(tr, sub.vec.cpu().numpy(), turns=2, sample=int(idx.numel()),
+                              variant=sub.var.cpu().numpy())
+            sub.track(tr, nt - early, early)
+        finally:
+            tr.set_tuning(**saved)
         b.state[idx] = sub.state
         b.ixt[idx] = sub.ixt
         b.ixe[idx] = sub.ixe
@@ -405,12 +408,14 @@ def pruned_scan(pb: ScanProblem, net: SurvivalMLP, v_begin: int, v_end: int, ear
     if m:
         sub = b.subset(idx)
         saved = tr.get_tuning()
-        if retune_subset:
-            from . import autotune
+        try:
+            if retune_subset:
+                from . import autotune
 
-            autotune.tune(tr, sub.vec.cpu().numpy(), turns=2, sample=m, variant=sub.var.cpu().numpy())
-        sub.track(tr, nt - early, early)
-        tr.set_tuning(**saved)
+                autotune.tune(tr, sub.vec.cpu().numpy(), turns=2, sample=m, variant=sub.var.cpu().numpy())
+            sub.track(tr, nt - early, early)
+        finally:
+            tr.set_tuning(**saved)
         actual[b.order[idx]] = sub.state == 1
         tracked_turns = int((survive_turns(sub.state, sub.ixt, nt) - early).clamp(min=0).sum().item())
     early_turns = int(torch.clamp(survive_turns(b.state, b.ixt, early), max=early).sum().item())
